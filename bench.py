@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark: D32 oscillating-sphere steps/s on B200 (and the CPU reference arm).
+
+Workload: the D = 32 oscillating sphere -- three nested levels (half widths
+2D, 4D, 8D: a 16D cube of 5,767,168 cells, 17,548,032 edges), A = 0.2 D,
+Re0 = 0.2, omega = 3.6, 200 steps per period, 3217 Fibonacci markers, closed
+no-slip cavity, float64.  A step is one ``Driver.step`` (4 Picard passes, each
+with a PCG solve to the reference's mixed 1e-10/1e-9 criterion checked every
+20 iterations).  Data are synthetic (the analytic sphere and its prescribed
+motion); nothing is read from disk.
+
+``value``    steps/s from CUDA events on the library stream over K steps,
+             fields resident in HBM (the prescribed marker positions of each
+             step, 154 KB, are its only host input).
+``e2e``      the same K steps through the public driver API (``SphereRun.advance``)
+             with the marker positions uploaded and the body load read back
+             every step, host wall clock.
+``roofline`` the PCG iteration: 80 algorithmic bytes per edge per iteration
+             (10 float64 edge streams) over its CUDA-event time, against the
+             measured HBM copy bandwidth.
+``cpu_baseline`` / ``--impl reference``: the NumPy restatement of the
+             reference's CPU path (oracle/) timed on the host on a bounded
+             sample (see ``reference_sample``).
+
+Multi-GPU: a single case does not shard (every CG iteration has global
+reductions); ``--gpus N`` under torchrun runs N independent replicas with no
+collective on the data path and reports the sum of their throughputs.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ALGO_BYTES_PER_EDGE_ITER = 80.0     # 10 float64 edge streams per PCG iteration
+ALGO_BYTES_PER_EDGE_MATVEC = 16.0   # read p, write w
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def maybe_init_dist(world, local, backend="nccl"):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def reduce_max(dist, value, device=None):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(dist, value, device=None):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference arm: the oracle (NumPy restatement of the reference CPU path)
+# ---------------------------------------------------------------------------
+def reference_sample(case, iters_per_step, cg_iters=6, threads=None):
+    """Time the oracle on a bounded sample and scale to one step of ``case``.
+
+    The sample runs the oracle's stencils (calc_vel, conv_diff, rot(integr_c2f))
+    and ``cg_iters`` PCG iterations (matrix-free flow_mat + vector updates, the
+    reference's CPU algorithm) on the same three-level oscillating-sphere
+    layout at D = 8 cells (92,160 cells; the full D = 32 layout needs several
+    minutes and ~20 GB just to assemble the oracle's geometry).  Costs are
+    scaled to the full layout by edge count (per-edge work is the same) and
+    to one step by the CG iteration count per step of the full case.
+    """
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyib_oracle as O
+    from pyib_b200.cases import SphereCase
+    small = SphereCase(name="sample", cells_per_diameter=8, half_widths_d=case.half_widths_d,
+                       reynolds=case.reynolds, amplitude_d=case.amplitude_d)
+    lay = small.layout().build()
+    desc, _ = lay.export_mesh()
+    m = O.MeshDesc(**desc)
+    drv = O.OracleDriver(m, small.viscosity, small.density, cavity=True)
+    ne_small = m.E2N.shape[0]
+    ne_full = full_edge_count(case)
+    rng = np.random.default_rng(0)
+    s = rng.standard_normal(ne_small) * 1e-3
+    dt = small.time_step
+    t0 = time.perf_counter()
+    for _ in range(6):
+        s2, U, vc = drv.calc_vel(s)
+    for _ in range(5):
+        drv.conv_diff(U, vc)
+    for _ in range(4):
+        drv.g.rot(drv.g.integr_c2f(vc[:m.ncell]))
+    t_stencil = time.perf_counter() - t0
+    p = rng.standard_normal(ne_small)
+    r = rng.standard_normal(ne_small)
+    x = np.zeros(ne_small)
+    t0 = time.perf_counter()
+    for _ in range(cg_iters):
+        w = drv.apply(p, dt)
+        w[drv.dir_mask] = 0.0
+        a = 1e-3 / max(p.dot(w), 1e-300)
+        x += a * p
+        r -= a * w
+        z = r * drv.prec
+        e = z.dot(r)
+        p = z + 0.5 * p
+    t_iter = (time.perf_counter() - t0) / cg_iters
+    scale = ne_full / ne_small
+    t_step = scale * (t_stencil + iters_per_step * t_iter)
+    sample = (f"oracle on the same 3-level layout at D=8 ({m.ncell} cells, {ne_small} edges): "
+              f"6 calc_vel + 5 conv_diff + 4 rot(integr) = {t_stencil:.2f}s and {cg_iters} PCG "
+              f"iterations at {t_iter*1e3:.1f} ms each; scaled x{scale:.1f} by edges and to "
+              f"{iters_per_step:.0f} CG iterations per step")
+    return 1.0 / t_step, sample
+
+
+def full_edge_count(case):
+    """Existing edges of a concentric nested layout (closed form, no tables).
+
+    A level box of n^3 cells has 3 n (n+1)^2 edges; the edges of the closed
+    hole box (m = n_inner / 2 cells a side) are absent (inside the hole) or
+    belong to the finer level (on the hole surface).
+    """
+    n = [int(round(2 * w * case.cells_per_diameter / 2 ** L)) for L, w in enumerate(case.half_widths_d)]
+    tot = 0
+    for L, nL in enumerate(n):
+        tot += 3 * nL * (nL + 1) ** 2
+        if L > 0:
+            m = n[L - 1] // 2
+            tot -= 3 * m * (m + 1) ** 2
+    return tot
+
+
+def cores_used():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# D32 FP64 CG iterations per step after the 3 warm-up steps (steps 4-13),
+# measured by the b200 arm; the oracle follows the same iterates (parity tests).
+D32_ITERS_PER_STEP = 1800.0
+
+
+def run_reference(args, world, rank):
+    from pyib_b200.cases import CASES
+    case = CASES[args.workload]
+    if rank != 0:
+        return 0
+    vals = []
+    sample = ""
+    for k in range(args.warmup + args.steps):
+        v, sample = reference_sample(case, D32_ITERS_PER_STEP, cg_iters=2)
+        if k >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": "D32 sphere steps/s", "value": value, "unit": "steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": case.name, "cells": 5767168, "levels": 3, "markers": 3217,
+                   "precision": "float64", "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args, world, rank, local):
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    from pyib_b200 import _lib, build
+    from pyib_b200.cases import CASES
+    from pyib_b200.runner import SphereRun
+
+    build.build_library()
+    dist = maybe_init_dist(world, local)
+    case = CASES[args.workload]
+    t_setup = time.perf_counter()
+    run = SphereRun(case, device=local if world > 1 else 0)
+    drv = run.drv
+    sv = drv.solver
+    setup_s = time.perf_counter() - t_setup
+    for _ in range(args.warmup):
+        run.advance()
+    barrier(dist)
+    sampler = ClockSampler(local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+    sampler.start()
+    timing = (C.c_double * 3)()
+    sv.h.call("pyib_cg_timing", timing, 1)
+    iters = []
+    ev_ms = C.c_double(0.0)
+    sv.h.call("pyib_event", 0, None)
+    for _ in range(args.steps):
+        k = run.step_index + 1
+        drv.time = (k - 1) * run.dt
+        run.s, run.vc, run.s_old = drv.step(run.s, run.s_old, run.dt, run.dt, inner=4)
+        drv.time = k * run.dt
+        run.step_index = k
+        iters.append(drv.helmholtz_total_iterations_last_step)
+    sv.h.call("pyib_event", 1, C.byref(ev_ms))
+    sv.h.call("pyib_cg_timing", timing, 1)
+    cg_s, cg_it, launches = float(timing[0]), float(timing[1]), int(timing[2])
+    t_dev = ev_ms.value / 1000.0
+    barrier(dist)
+    # e2e: public API, host inputs and a host read of the step's load every step
+    run.loads.initialize(run.centre(drv.time))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        load = run.advance()
+        _ = float(load["body_force"][0])
+    t_e2e = time.perf_counter() - t0
+    clocks = sampler.stop()
+    # standalone matvec timing
+    mv_ms = C.c_double(0.0)
+    sv.set("WORK_E", np.random.default_rng(0).standard_normal(sv.lay.NE) * sv.lay.edge_exists)
+    sv.h.call("pyib_bench_matvec", 50, C.c_double(run.dt), C.byref(mv_ms))
+    ne = int(sv.lay.edge_exists.sum())
+    t_dev_max = reduce_max(dist, t_dev)
+    t_e2e_max = reduce_max(dist, t_e2e)
+    total_steps = args.steps * world
+    value = total_steps / t_dev_max
+    e2e = total_steps / t_e2e_max
+    peak, peak_kind = peaks()
+    t_iter = cg_s / max(cg_it, 1.0)
+    achieved = ALGO_BYTES_PER_EDGE_ITER * ne / t_iter / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "cg_iteration_d32_traffic.json"
+    if tf.exists():
+        d = json.loads(tf.read_text())
+        traffic = d.get("bytes_per_edge_iteration", 0.0) * ne
+    mv_achieved = ALGO_BYTES_PER_EDGE_MATVEC * ne / (mv_ms.value / 1e3) / 1e9
+    M = drv.ib_markers.shape[0]
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, sample = reference_sample(case, float(np.mean(iters)), cg_iters=3)
+            cpu = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample}
+        line = {
+            "metric": "D32 sphere steps/s", "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": case.name, "cells": int(sv.lay.cell_active.sum()), "edges": ne,
+                       "levels": sv.lay.N, "markers": M, "precision": "float64",
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (working set > 2 GB)",
+                       "cg_iterations_per_step": float(np.mean(iters)), "setup_seconds": setup_s},
+            "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 2 * 3 * M * 8,
+                    "d2h_bytes_per_step": 13 * 8},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "PCG iteration (matvec A/V/RI + update + direction)",
+                         "algorithmic_bytes_per_launch": ALGO_BYTES_PER_EDGE_ITER * ne,
+                         "peak_kind": peak_kind},
+            "matvec": {"ms": mv_ms.value, "achieved_gbs": mv_achieved, "frac": mv_achieved / peak,
+                       "algorithmic_bytes": ALGO_BYTES_PER_EDGE_MATVEC * ne},
+            "cg": {"seconds": cg_s, "iterations": cg_it, "ms_per_iteration": 1e3 * t_iter,
+                   "gbs": achieved},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="d32_oscillating_sphere")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,97 @@
+"""Exact incidence operators of the nested layout as sparse matrices (host, built once).
+
+All matrices use the dense ids of :mod:`layout` and the +a orientation of
+faces and edges.  They restate, row for row, the reference's operators
+(``ib_core_np.py:129-183``) in that orientation:
+
+* ``C``    curl, edges -> faces          (``IBCore.curl``, ib_core_np.py:133)
+* ``R``    rot = C^T, faces -> edges     (``IBCore.rot``, ib_core_np.py:129)
+* ``P[d]`` interp_f2c component d        (ib_core_np.py:150-157)
+* ``I[d]`` integr_c2f component d        (ib_core_np.py:144-148)
+* ``D``    cdiv, faces -> cells          (ib_core_np.py:136-139)
+* ``G0``   cgrad with zero ghost         (ib_core_np.py:177-183)
+* ``Vd``   vol * D * diag(AoL) * G0, the viscous block of ``flow_mat``
+  (ib_core_np.py:168-175) without the ``-0.5*dt*visc`` factor
+
+These are the ground truth the GPU templates are checked against; rows the
+structured templates cannot reproduce become explicit patch rows.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+
+class Operators:
+    def __init__(self, lay):
+        if not getattr(lay, "_built", False):
+            lay.build()
+        self.lay = lay
+        NC, NF, NE = lay.NC, lay.NF, lay.NE
+        self.C = sp.csr_matrix((lay.link_sign, (lay.link_face, lay.link_edge)), shape=(NF, NE))
+        self.C.sum_duplicates()
+        self.R = self.C.T.tocsr()
+        f = np.nonzero(lay.face_exists)[0]
+        lo, hi = lay.face_lo[f], lay.face_hi[f]
+        mlo, mhi = lo >= 0, hi >= 0
+        vol_ci = np.zeros(NC)
+        vol_ci[lay.cell_active] = 1.0 / lay.cell_vol[lay.cell_active]
+        self.vol_ci = vol_ci
+        dlo = lay.fpos[f[mlo]] - lay.cpos[lo[mlo]]
+        dhi = lay.fpos[f[mhi]] - lay.cpos[hi[mhi]]
+        self.P, self.I = [], []
+        for d in range(3):
+            rows = np.concatenate([lo[mlo], hi[mhi]])
+            cols = np.concatenate([f[mlo], f[mhi]])
+            vals = np.concatenate([vol_ci[lo[mlo]] * dlo[:, d], -vol_ci[hi[mhi]] * dhi[:, d]])
+            self.P.append(sp.csr_matrix((vals, (rows, cols)), shape=(NC, NF)))
+            self.I.append(sp.csr_matrix((np.concatenate([dlo[:, d], -dhi[:, d]]), (cols, rows)),
+                                        shape=(NF, NC)))
+        self.D = sp.csr_matrix((np.concatenate([np.ones(mlo.sum()), -np.ones(mhi.sum())]),
+                                (np.concatenate([lo[mlo], hi[mhi]]), np.concatenate([f[mlo], f[mhi]]))),
+                               shape=(NC, NF))
+        self.G0 = sp.csr_matrix((np.concatenate([-np.ones(mlo.sum()), np.ones(mhi.sum())]),
+                                 (np.concatenate([f[mlo], f[mhi]]), np.concatenate([lo[mlo], hi[mhi]]))),
+                                shape=(NF, NC))
+        self.AoL = lay.face_AoL()
+        self.Vd = (sp.diags(vol_ci) @ self.D @ sp.diags(self.AoL) @ self.G0).tocsr()
+
+    # ---- boundary conditions (ib_driver_np.py:120-121, 155-166) -----------
+    def dir_mask(self, cavity):
+        lay = self.lay
+        if cavity:
+            m = lay.edge_bc > 0
+        else:
+            m = np.isin(lay.edge_bc, (3, 4, 5, 6))
+        return m
+
+    def inlet_mask(self, cavity):
+        if cavity:
+            return np.zeros(self.lay.NE, dtype=bool)
+        return self.lay.edge_bc == 1
+
+    def prec(self, dir_mask):
+        """Geometric diagonal preconditioner, ib_driver_np.py:78-88 (0 on Dirichlet/absent edges)."""
+        lay = self.lay
+        rf = lay.face_rf()
+        ax = lay.face_axis.astype(np.int64)
+        q = np.zeros(lay.NF)
+        ok = lay.face_exists
+        q[ok] = rf[ok, ax[ok]] / lay.face_Af[ok]            # (rf.nf)/Af^2 with nf = Af e_a
+        d = np.bincount(lay.link_edge, weights=q[lay.link_face], minlength=lay.NE)
+        d[dir_mask | ~lay.edge_exists] = 0.0
+        out = np.zeros(lay.NE)
+        nz = d != 0.0
+        out[nz] = 1.0 / d[nz]
+        return out
+
+    # ---- composite operators ---------------------------------------------
+    def V(self, rou, visc, dt):
+        return (rou * sp.identity(self.lay.NC, format="csr") - (0.5 * dt * visc) * self.Vd).tocsr()
+
+    def flow_mat(self, p, alpd=0.0, visc=0.0, rou=1.0, dt=0.0):
+        U = self.C @ p
+        v = [self.P[d] @ U for d in range(3)]
+        if alpd != 0.0:
+            v = [rou * vd - (0.5 * dt * visc) * (self.Vd @ vd) for vd in v]
+        return self.R @ sum(self.I[d] @ v[d] for d in range(3))
