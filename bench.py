@@ -278,7 +278,8 @@ def run_b200(args, world, rank, local):
     dist = maybe_init_dist(world, local)
     case = CASES[args.workload]
     t_setup = time.perf_counter()
-    run = SphereRun(case, device=local if world > 1 else 0)
+    run = SphereRun(case, device=local if world > 1 else 0, precision=args.precision,
+                    mixed_tol=args.mixed_tol)
     drv = run.drv
     sv = drv.solver
     setup_s = time.perf_counter() - t_setup
@@ -343,7 +344,7 @@ def run_b200(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": case.name, "cells": int(sv.lay.cell_active.sum()), "edges": ne,
-                       "levels": sv.lay.N, "markers": M, "precision": "float64",
+                       "levels": sv.lay.N, "markers": M, "precision": args.precision,
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (working set > 2 GB)",
                        "cg_iterations_per_step": float(np.mean(iters)), "setup_seconds": setup_s},
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 2 * 3 * M * 8,
@@ -376,6 +377,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="d32_oscillating_sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="float64", choices=["float64", "mixed"])
+    ap.add_argument("--mixed-tol", type=float, default=1e-4)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -32,7 +32,7 @@ T = {name: i for i, name in enumerate(TABLES)}
 
 FIELDS = [
     "S", "S_OLD", "U", "VC", "VC_GHOST", "RES_C", "RES_E", "FE", "FL", "MARKERS", "MVEL", "DS",
-    "WORK_E", "WORK_E2", "WORK_C3", "WORK_F", "IB_CELL", "IB_W", "IB_BASE", "LAG_TMP",
+    "WORK_E", "WORK_E2", "WORK_C3", "WORK_F", "IB_CELL", "IB_W", "IB_BASE", "LAG_TMP", "DINV",
 ]
 F = {name: i for i, name in enumerate(FIELDS)}
 
@@ -65,6 +65,7 @@ class Params(C.Structure):
         ("cavity", C.c_int32), ("check", C.c_int32), ("cg_max", C.c_int32), ("strict", C.c_int32),
         ("precision", C.c_int32), ("nmarkers", C.c_int32),
         ("hh", C.c_double), ("hh3", C.c_double),
+        ("mixed_tol", C.c_double), ("mixed_max_sweeps", C.c_int32), ("pad", C.c_int32),
     ]
 
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -27,8 +28,12 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxBlocks = 148 * 8;      // fixed reduction grid (148 SMs x 8)
+constexpr int kMaxBlocks = 148 * 8;      // fixed grid of the flat vector kernels (148 SMs x 8)
+constexpr int kPartStride = 32768;       // partial-sum slots per reduction value (>= any grid)
 constexpr int kSlots = 16;               // reduction values per block
+// structured stencil tiles: 32 x 8 threads in (x, y), each marching KZ planes in z
+constexpr int TX = 32, TY = 8;
+constexpr int kTargetBlocks = 148 * 16;   // z-chunk depth is chosen to give at least this many tiles
 
 struct LevelMeta {
   int n[3];
@@ -40,18 +45,24 @@ struct LevelMeta {
   long long fbase[3];
   long long ebase[3];
   long long ecount[3];
+  int zbA;             // first z-block of this level in the cell-tile grids
+  int zbR;             // first z-block of this level in the node-tile grid
 };
 
 struct Meta {
   int nl;
   LevelMeta lv[PYIB_MAX_LEVELS];
   long long nc, nf, ne;
+  int kz;              // z planes marched by one tile
+  int gxA, gyA, gzA;   // cell-tile grid (kernels A and V)
+  int gxR, gyR, gzR;   // node-tile grid (kernel RI), tiles of (TX-1) x (TY-1) nodes
 };
 
 struct CGState {
   double eta, eta_new, pw, alpha, beta, thresh, l2_0, xnorm;
   double true_eta, true_l2, tol1, tol2;
   double rou, kfac;              // V block: rou*v - kfac*(Vd v)
+  double thresh_in;              // inner (float32) stop threshold of the mixed solver
   int m, done, iters, check, cg_max, alpd, pad0, pad1;
   unsigned int counter;
   unsigned int pad2;
@@ -85,6 +96,12 @@ struct pyib_ctx {
          *prev = nullptr;
   float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *w32 = nullptr, *vcm32 = nullptr,
         *vq32 = nullptr, *prec32 = nullptr;
+  float *pa_val32 = nullptr, *pv_val32 = nullptr, *pr_val32 = nullptr;
+  double *diag1 = nullptr, *diag2 = nullptr;   // diag(R I P C) and diag(R I Vd' P C)
+  double diag_for_kfac = -1.0, diag_for_rou = -1.0;
+  bool diag_ready = false;
+  cudaGraphExec_t mix_graph = nullptr;
+  int mix_graph_check = 0;
   // reduction / state
   double* partials = nullptr;
   CGState* st = nullptr;
@@ -161,7 +178,8 @@ int grid_for(long long n) {
 // ---------------------------------------------------------------------------
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /*[NV*32]*/) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int lane = tid & 31, wid = tid >> 5;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double t = v[q];
@@ -170,7 +188,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /*[NV*32]*
   }
   __syncthreads();
   if (wid == 0) {
-    const int nw = blockDim.x >> 5;
+    const int nw = (blockDim.x * blockDim.y * blockDim.z) >> 5;
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double t = lane < nw ? sh[q * 32 + lane] : 0.0;
@@ -188,12 +206,16 @@ __device__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counte
   __shared__ double sh[NV * 32];
   __shared__ bool last;
   block_sum<NV>(v, sh);
-  if (threadIdx.x == 0) {
+  const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthr = blockDim.x * blockDim.y * blockDim.z;
+  if (tid == 0) {
 #pragma unroll
-    for (int q = 0; q < NV; ++q) partials[q * kMaxBlocks + blockIdx.x] = v[q];
+    for (int q = 0; q < NV; ++q) partials[q * kPartStride + bid] = v[q];
     __threadfence();
     unsigned int t = atomicAdd(counter, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == nb - 1);
   }
   __syncthreads();
   if (!last) return false;
@@ -202,42 +224,40 @@ __device__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counte
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double t = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-      t += ((volatile double*)partials)[q * kMaxBlocks + b];
+    for (unsigned int b = tid; b < nb; b += nthr) t += ((volatile double*)partials)[q * kPartStride + b];
     acc[q] = t;
   }
   block_sum<NV>(acc, sh);
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = acc[q];
     *counter = 0u;
   }
-  return true;
+  return tid == 0;
 }
 
 // ---------------------------------------------------------------------------
 // layout decoding
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int level_of_cell(const Meta& m, long long c) {
-  int L = 0;
-  while (L + 1 < m.nl && c >= m.lv[L + 1].cbase) ++L;
-  return L;
-}
 
-__device__ __forceinline__ bool in_hole(const LevelMeta& l, int i, int j, int k) {
-  return l.has_hole && i >= l.hole_lo[0] && i < l.hole_hi[0] && j >= l.hole_lo[1] &&
-         j < l.hole_hi[1] && k >= l.hole_lo[2] && k < l.hole_hi[2];
-}
 
 __device__ __forceinline__ bool bit_set(const unsigned int* bits, long long i) {
   return (bits[i >> 5] >> (i & 31)) & 1u;
 }
 
+__device__ __forceinline__ int level_of_zblock(const Meta& m, int bz, bool node_grid) {
+  int L = 0;
+  while (L + 1 < m.nl && bz >= (node_grid ? m.lv[L + 1].zbR : m.lv[L + 1].zbA)) ++L;
+  return L;
+}
+
 // ---------------------------------------------------------------------------
-// matvec kernel A: vc = P C p (template + patch)
+// matvec kernel A: vc = P C p.  Thread (i,j) of a 32x8 tile marches KZ cell planes;
+// the two x- and y-edge values of the upper plane are carried to the next plane.
+// Irregular cells (hole neighbours, interface cells) take their exact CSR rows.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_mvA(Meta m, const T* __restrict__ p, T* __restrict__ vc,
+__global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p, T* __restrict__ vc,
                                                   const unsigned int* __restrict__ pbits,
                                                   const int* __restrict__ prow,
                                                   const long long* __restrict__ pptr,
@@ -245,53 +265,63 @@ __global__ void __launch_bounds__(kThreads) k_mvA(Meta m, const T* __restrict__ 
                                                   const T* __restrict__ pval, long long nA,
                                                   const CGState* __restrict__ st) {
   if (st && st->done) return;
+  const int L = level_of_zblock(m, blockIdx.z, false);
+  const LevelMeta& l = m.lv[L];
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
+  if (i >= nx || j >= ny) return;
+  const int k0 = (blockIdx.z - l.zbA) * m.kz;
+  const int k1 = min(k0 + m.kz, nz);
   const long long nc = m.nc;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
-       c += (long long)gridDim.x * blockDim.x) {
-    const int L = level_of_cell(m, c);
-    const LevelMeta& l = m.lv[L];
-    const int nx = l.n[0], ny = l.n[1];
-    int loc = (int)(c - l.cbase);
-    const int i = loc % nx, j = (loc / nx) % ny, k = loc / (nx * ny);
-    if (in_hole(l, i, j, k)) continue;
-    if (pbits && bit_set(pbits, c)) {
-      const int r = prow[c];
-      for (int d = 0; d < 3; ++d) {
-        T acc = 0;
-        const long long rr = r + d * nA;
-        for (long long q = pptr[rr]; q < pptr[rr + 1]; ++q) acc += pval[q] * p[pcol[q]];
-        vc[d * nc + c] = acc;
+  const T* ex = p + l.ebase[0];
+  const T* ey = p + l.ebase[1];
+  const T* ez = p + l.ebase[2];
+  const int sxk = (ny + 1) * nx, syk = ny * (nx + 1), szk = (ny + 1) * (nx + 1);
+  int ox = (k0 * (ny + 1) + j) * nx + i;
+  int oy = (k0 * ny + j) * (nx + 1) + i;
+  int oz = (k0 * (ny + 1) + j) * (nx + 1) + i;
+  T ex00 = ex[ox], ex10 = ex[ox + nx];
+  T ey00 = ey[oy], ey10 = ey[oy + 1];
+  const T s = (T)(1.0 / (2.0 * l.h * l.h));
+  const bool col_hole = l.has_hole && i >= l.hole_lo[0] && i < l.hole_hi[0] && j >= l.hole_lo[1] &&
+                        j < l.hole_hi[1];
+  long long c = l.cbase + ((long long)k0 * ny + j) * nx + i;
+  const long long cstep = (long long)nx * ny;
+  for (int k = k0; k < k1; ++k, c += cstep, ox += sxk, oy += syk, oz += szk) {
+    const T ex01 = ex[ox + sxk], ex11 = ex[ox + sxk + nx];
+    const T ey01 = ey[oy + syk], ey11 = ey[oy + syk + 1];
+    if (!(col_hole && k >= l.hole_lo[2] && k < l.hole_hi[2])) {
+      if (pbits && bit_set(pbits, c)) {
+        const int r = prow[c];
+        for (int d = 0; d < 3; ++d) {
+          T acc = 0;
+          const long long rr = r + d * nA;
+          for (long long q = pptr[rr]; q < pptr[rr + 1]; ++q) acc += pval[q] * p[pcol[q]];
+          vc[d * nc + c] = acc;
+        }
+      } else {
+        const T ez00 = ez[oz], ez10 = ez[oz + 1], ez01 = ez[oz + nx + 1], ez11 = ez[oz + nx + 2];
+        const T ux0 = ey00 + ez01 - ey01 - ez00;
+        const T ux1 = ey10 + ez11 - ey11 - ez10;
+        const T uy0 = ez00 + ex01 - ez10 - ex00;
+        const T uy1 = ez01 + ex11 - ez11 - ex10;
+        const T uz0 = ex00 + ey10 - ex10 - ey00;
+        const T uz1 = ex01 + ey11 - ex11 - ey01;
+        vc[c] = (ux0 + ux1) * s;
+        vc[nc + c] = (uy0 + uy1) * s;
+        vc[2 * nc + c] = (uz0 + uz1) * s;
       }
-      continue;
     }
-    const T* ex = p + l.ebase[0];
-    const T* ey = p + l.ebase[1];
-    const T* ez = p + l.ebase[2];
-    // x-edges dims (nx, ny+1, nz+1); y-edges (nx+1, ny, nz+1); z-edges (nx+1, ny+1, nz)
-    auto EX = [&](int a, int b, int cc) { return ex[((long long)cc * (ny + 1) + b) * nx + a]; };
-    auto EY = [&](int a, int b, int cc) { return ey[((long long)cc * ny + b) * (nx + 1) + a]; };
-    auto EZ = [&](int a, int b, int cc) { return ez[((long long)cc * (ny + 1) + b) * (nx + 1) + a]; };
-    const T ex00 = EX(i, j, k), ex10 = EX(i, j + 1, k), ex01 = EX(i, j, k + 1), ex11 = EX(i, j + 1, k + 1);
-    const T ey00 = EY(i, j, k), ey10 = EY(i + 1, j, k), ey01 = EY(i, j, k + 1), ey11 = EY(i + 1, j, k + 1);
-    const T ez00 = EZ(i, j, k), ez10 = EZ(i + 1, j, k), ez01 = EZ(i, j + 1, k), ez11 = EZ(i + 1, j + 1, k);
-    const T ux0 = ey00 + ez01 - ey01 - ez00;
-    const T ux1 = ey10 + ez11 - ey11 - ez10;
-    const T uy0 = ez00 + ex01 - ez10 - ex00;
-    const T uy1 = ez01 + ex11 - ez11 - ex10;
-    const T uz0 = ex00 + ey10 - ex10 - ey00;
-    const T uz1 = ex01 + ey11 - ex11 - ey01;
-    const T s = (T)(1.0 / (2.0 * l.h * l.h));
-    vc[c] = (ux0 + ux1) * s;
-    vc[nc + c] = (uy0 + uy1) * s;
-    vc[2 * nc + c] = (uz0 + uz1) * s;
+    ex00 = ex01; ex10 = ex11; ey00 = ey01; ey10 = ey11;
   }
 }
 
 // ---------------------------------------------------------------------------
-// matvec kernel V: vq = rou v - kfac * Vd v  (per component; template + patch)
+// matvec kernel V: vq = rou v - kfac * Vd v per component (7-point template with a
+// zero ghost at the domain boundary); the z-neighbours are carried in registers.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_mvV(Meta m, const T* __restrict__ v, T* __restrict__ vq,
+__global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v, T* __restrict__ vq,
                                                   const unsigned int* __restrict__ pbits,
                                                   const int* __restrict__ prow,
                                                   const long long* __restrict__ pptr,
@@ -299,65 +329,70 @@ __global__ void __launch_bounds__(kThreads) k_mvV(Meta m, const T* __restrict__ 
                                                   const T* __restrict__ pval,
                                                   const CGState* __restrict__ st) {
   if (st->done) return;
+  const int L = level_of_zblock(m, blockIdx.z, false);
+  const LevelMeta& l = m.lv[L];
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
+  if (i >= nx || j >= ny) return;
+  const int k0 = (blockIdx.z - l.zbA) * m.kz;
+  const int k1 = min(k0 + m.kz, nz);
   const long long nc = m.nc;
   const T rou = (T)st->rou, kf = (T)st->kfac;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
-       c += (long long)gridDim.x * blockDim.x) {
-    const int L = level_of_cell(m, c);
-    const LevelMeta& l = m.lv[L];
-    const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
-    int loc = (int)(c - l.cbase);
-    const int i = loc % nx, j = (loc / nx) % ny, k = loc / (nx * ny);
-    if (in_hole(l, i, j, k)) continue;
-    if (pbits && bit_set(pbits, c)) {
-      const int r = prow[c];
-      for (int d = 0; d < 3; ++d) {
-        T acc = 0;
-        const T* vd = v + d * nc;
-        for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vd[pcol[q]];
-        vq[d * nc + c] = rou * vd[c] - kf * acc;
+  const T inv_h2 = (T)(1.0 / (l.h * l.h));
+  const long long cstep = (long long)nx * ny;
+  const long long c0 = l.cbase + ((long long)k0 * ny + j) * nx + i;
+  const bool col_hole = l.has_hole && i >= l.hole_lo[0] && i < l.hole_hi[0] && j >= l.hole_lo[1] &&
+                        j < l.hole_hi[1];
+  const bool xm = i > 0, xp = i + 1 < nx, ym = j > 0, yp = j + 1 < ny;
+  T vm[3], v0[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    v0[d] = v[d * nc + c0];
+    vm[d] = k0 > 0 ? v[d * nc + c0 - cstep] : (T)0;
+  }
+  long long c = c0;
+  for (int k = k0; k < k1; ++k, c += cstep) {
+    T vp[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) vp[d] = k + 1 < nz ? v[d * nc + c + cstep] : (T)0;
+    if (!(col_hole && k >= l.hole_lo[2] && k < l.hole_hi[2])) {
+      if (pbits && bit_set(pbits, c)) {
+        const int r = prow[c];
+        for (int d = 0; d < 3; ++d) {
+          T acc = 0;
+          const T* vd = v + d * nc;
+          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vd[pcol[q]];
+          vq[d * nc + c] = rou * v0[d] - kf * acc;
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const T* vd = v + d * nc;
+          const T vc0 = v0[d];
+          T acc = 0;
+          acc += xp ? vd[c + 1] - vc0 : -2 * vc0;
+          acc += xm ? vd[c - 1] - vc0 : -2 * vc0;
+          acc += yp ? vd[c + nx] - vc0 : -2 * vc0;
+          acc += ym ? vd[c - nx] - vc0 : -2 * vc0;
+          acc += (k + 1 < nz) ? vp[d] - vc0 : -2 * vc0;
+          acc += (k > 0) ? vm[d] - vc0 : -2 * vc0;
+          vq[d * nc + c] = rou * vc0 - kf * (acc * inv_h2);
+        }
       }
-      continue;
     }
-    const T inv_h2 = (T)(1.0 / (l.h * l.h));
-    const long long sx = 1, sy = nx, sz = (long long)nx * ny;
-    for (int d = 0; d < 3; ++d) {
-      const T* vd = v + d * nc;
-      const T vc0 = vd[c];
-      T acc = 0;
-      acc += (i + 1 < nx) ? vd[c + sx] - vc0 : -2 * vc0;
-      acc += (i > 0) ? vd[c - sx] - vc0 : -2 * vc0;
-      acc += (j + 1 < ny) ? vd[c + sy] - vc0 : -2 * vc0;
-      acc += (j > 0) ? vd[c - sy] - vc0 : -2 * vc0;
-      acc += (k + 1 < nz) ? vd[c + sz] - vc0 : -2 * vc0;
-      acc += (k > 0) ? vd[c - sz] - vc0 : -2 * vc0;
-      vq[d * nc + c] = rou * vc0 - kf * (acc * inv_h2);
-    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { vm[d] = v0[d]; v0[d] = vp[d]; }
   }
 }
 
 // ---------------------------------------------------------------------------
-// matvec kernel RI: w = R I vq (template + patch), fused dot p.w, alpha
+// matvec kernel RI: w = R I vq, fused with the dot p.w and alpha = eta / p.w.
+// A 32x8 block covers (TX-1)x(TY-1) node columns plus a one-node halo at -x,-y; each
+// thread forms the three face values F_a = (h/2)(vq_a[lo] + vq_a[hi]) at its node
+// index, shares them through a shared-memory plane, and marches KZ planes in z.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ T face_F(const LevelMeta& l, const T* __restrict__ vq, long long nc, int a,
-                                    int fi, int fj, int fk) {
-  // F on the a-face at (fi,fj,fk): (h/2)(vq_a[lo cell] + vq_a[hi cell]); zero outside the box
-  if (fi < 0 || fj < 0 || fk < 0) return 0;
-  if (fi >= l.n[0] + (a == 0) || fj >= l.n[1] + (a == 1) || fk >= l.n[2] + (a == 2)) return 0;
-  const T* va = vq + a * nc + l.cbase;
-  const long long sy = l.n[0], sz = (long long)l.n[0] * l.n[1];
-  const int fa = a == 0 ? fi : (a == 1 ? fj : fk);
-  const long long off = fk * sz + fj * sy + fi;
-  const long long sa = a == 0 ? 1 : (a == 1 ? sy : sz);
-  T s = 0;
-  if (fa > 0) s += va[off - sa];          // lo cell = f - e_a
-  if (fa < l.n[a]) s += va[off];          // hi cell = f
-  return (T)(0.5 * l.h) * s;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
+__global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
                                                    const T* __restrict__ p,
                                                    const unsigned int* __restrict__ pbits,
                                                    const int* __restrict__ prow,
@@ -366,42 +401,107 @@ __global__ void __launch_bounds__(kThreads) k_mvRI(Meta m, const T* __restrict__
                                                    const T* __restrict__ pval, double* partials,
                                                    CGState* st, int do_dot) {
   if (st->done) return;
-  const long long ne = m.ne, nc = m.nc;
+  __shared__ T sF[2][3][TY][TX];
+  const int L = level_of_zblock(m, blockIdx.z, true);
+  const LevelMeta& l = m.lv[L];
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * (TX - 1) + tx - 1, j = blockIdx.y * (TY - 1) + ty - 1;
+  const int k0 = (blockIdx.z - l.zbR) * m.kz;
+  const int k1 = min(k0 + m.kz, nz + 1);
+  const long long nc = m.nc;
+  const T* vx = vq + l.cbase;
+  const T* vy = vq + nc + l.cbase;
+  const T* vz = vq + 2 * nc + l.cbase;
+  const T hh = (T)(0.5 * l.h);
+  const int cs = nx * ny;
+  const bool in_ij = i >= 0 && j >= 0 && i <= nx && j <= ny;
+  const bool own = tx > 0 && ty > 0 && in_ij;
+  const bool cx = i < nx && j < ny;            // cell (i,j,.) exists in x,y
+  const bool cxm = i > 0 && j < ny;            // cell (i-1,j,.)
+  const bool cym = j > 0 && i < nx;            // cell (i,j-1,.)
+  // F at plane k0-1 for the own node (z-direction differences)
+  auto Fx = [&](int k) -> T {   // x-face at node (i,j,k): cells (i-1,j,k),(i,j,k)
+    if (!in_ij || k < 0 || k >= nz || j >= ny) return (T)0;
+    const int o = k * cs + j * nx + i;
+    T a = 0;
+    if (i > 0) a += vx[o - 1];
+    if (i < nx) a += vx[o];
+    return hh * a;
+  };
+  auto Fy = [&](int k) -> T {   // y-face at (i,j,k): cells (i,j-1,k),(i,j,k)
+    if (!in_ij || k < 0 || k >= nz || i >= nx) return (T)0;
+    const int o = k * cs + j * nx + i;
+    T a = 0;
+    if (j > 0) a += vy[o - nx];
+    if (j < ny) a += vy[o];
+    return hh * a;
+  };
+  (void)cx; (void)cxm; (void)cym;
+  T fx_prev = Fx(k0 - 1), fy_prev = Fy(k0 - 1);
+  // vz at (i,j,k0-1) for F_z
+  T vz_prev = (in_ij && i < nx && j < ny && k0 > 0) ? vz[(k0 - 1) * cs + j * nx + i] : (T)0;
   double dot[1] = {0.0};
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x) {
-    T val;
-    if (pbits && bit_set(pbits, e)) {
-      const int r = prow[e];
-      T acc = 0;
-      for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
-      val = acc;
-    } else {
-      int L = 0, t = 0;
-      for (;;) {
-        const LevelMeta& l = m.lv[L];
-        if (e < l.ebase[2] + l.ecount[2]) {
-          t = e >= l.ebase[2] ? 2 : (e >= l.ebase[1] ? 1 : 0);
-          break;
+  const int ex_sk = (ny + 1) * nx, ey_sk = ny * (nx + 1), ez_sk = (ny + 1) * (nx + 1);
+  int buf = 0;
+  for (int k = k0; k < k1; ++k) {
+    const T fx = Fx(k), fy = Fy(k);
+    T vz_cur = (in_ij && i < nx && j < ny && k < nz) ? vz[k * cs + j * nx + i] : (T)0;
+    const T fz = hh * (vz_prev + vz_cur);     // z-face at (i,j,k): cells (i,j,k-1),(i,j,k)
+    sF[buf][0][ty][tx] = fx;
+    sF[buf][1][ty][tx] = fy;
+    sF[buf][2][ty][tx] = fz;
+    __syncthreads();
+    if (own) {
+      // w_x(i,j,k) = Fz(i,j,k) - Fz(i,j-1,k) + Fy(i,j,k-1) - Fy(i,j,k)
+      // w_y(i,j,k) = Fx(i,j,k) - Fx(i,j,k-1) + Fz(i-1,j,k) - Fz(i,j,k)
+      // w_z(i,j,k) = Fy(i,j,k) - Fy(i-1,j,k) + Fx(i,j-1,k) - Fx(i,j,k)
+      const T fz_jm = sF[buf][2][ty - 1][tx], fz_im = sF[buf][2][ty][tx - 1];
+      const T fy_im = sF[buf][1][ty][tx - 1], fx_jm = sF[buf][0][ty - 1][tx];
+      if (i < nx) {
+        long long e = l.ebase[0] + (long long)k * ex_sk + j * nx + i;
+        T val = fz - fz_jm + fy_prev - fy;
+        if (pbits && bit_set(pbits, e)) {
+          const int r = prow[e];
+          T acc = 0;
+          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
+          val = acc;
         }
-        ++L;
+        w[e] = val;
+        if (do_dot) dot[0] += (double)p[e] * (double)val;
       }
-      const LevelMeta& l = m.lv[L];
-      const int dx = l.n[0] + (t != 0), dy = l.n[1] + (t != 1);
-      const int loc = (int)(e - l.ebase[t]);
-      const int i = loc % dx, j = (loc / dx) % dy, k = loc / (dx * dy);
-      const int t1 = (t + 1) % 3, t2 = (t + 2) % 3;
-      int q1[3] = {i, j, k}, q2[3] = {i, j, k};
-      q1[t1] -= 1;   // idx - e_{t+1}
-      q2[t2] -= 1;   // idx - e_{t+2}
-      val = face_F<T>(l, vq, nc, t2, i, j, k) - face_F<T>(l, vq, nc, t2, q1[0], q1[1], q1[2]) +
-            face_F<T>(l, vq, nc, t1, q2[0], q2[1], q2[2]) - face_F<T>(l, vq, nc, t1, i, j, k);
+      if (j < ny) {
+        long long e = l.ebase[1] + (long long)k * ey_sk + j * (nx + 1) + i;
+        T val = fx - fx_prev + fz_im - fz;
+        if (pbits && bit_set(pbits, e)) {
+          const int r = prow[e];
+          T acc = 0;
+          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
+          val = acc;
+        }
+        w[e] = val;
+        if (do_dot) dot[0] += (double)p[e] * (double)val;
+      }
+      if (k < nz) {
+        long long e = l.ebase[2] + (long long)k * ez_sk + j * (nx + 1) + i;
+        T val = fy - fy_im + fx_jm - fx;
+        if (pbits && bit_set(pbits, e)) {
+          const int r = prow[e];
+          T acc = 0;
+          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
+          val = acc;
+        }
+        w[e] = val;
+        if (do_dot) dot[0] += (double)p[e] * (double)val;
+      }
     }
-    w[e] = val;
-    if (do_dot) dot[0] += (double)p[e] * (double)val;
+    fx_prev = fx;
+    fy_prev = fy;
+    vz_prev = vz_cur;
+    buf ^= 1;
   }
   if (!do_dot) return;
-  if (grid_sum<1>(dot, partials, &st->counter) && threadIdx.x == 0) {
+  if (grid_sum<1>(dot, partials, &st->counter)) {
     st->pw = dot[0];
     st->alpha = st->eta / (dot[0] != 0.0 ? dot[0] : INFINITY);
   }
@@ -517,6 +617,150 @@ __global__ void __launch_bounds__(kThreads) k_cg_true(long long ne, const double
   if (grid_sum<2>(v, partials, &st->counter) && threadIdx.x == 0) {
     st->true_eta = v[0];
     st->true_l2 = v[1];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// mixed precision: float32 PCG inside float64 iterative refinement
+// ---------------------------------------------------------------------------
+__global__ void k_d2f(long long n, const double* __restrict__ a, float* b) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    b[e] = (float)a[e];
+}
+
+// inner start: r32 = r64 (masked), d32 = 0, p32 = r32*dinv, eta = sum (r32*dinv)*r32
+__global__ void __launch_bounds__(kThreads) k_mix_start(long long ne, const double* __restrict__ r64,
+                                                        const float* __restrict__ dinv, float* r32,
+                                                        float* d32, float* p32, double eps_in2,
+                                                        double* partials, CGState* st) {
+  double v[1] = {0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    const float di = dinv[e];
+    const float re = di != 0.f ? (float)r64[e] : 0.f;
+    r32[e] = re;
+    d32[e] = 0.f;
+    const float pe = re * di;
+    p32[e] = pe;
+    v[0] += (double)pe * (double)re;
+  }
+  if (grid_sum<1>(v, partials, &st->counter)) {
+    st->eta = v[0];
+    st->thresh_in = eps_in2 * v[0];
+    st->m = 0;
+    st->done = v[0] > 0.0 ? 0 : 1;
+    st->iters = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_update32(long long ne, float* d32, float* r32,
+                                                          const float* __restrict__ p32,
+                                                          const float* __restrict__ w32,
+                                                          const float* __restrict__ dinv,
+                                                          double* partials, CGState* st) {
+  if (st->done) return;
+  const float alpha = (float)st->alpha;
+  double v[1] = {0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    const float di = dinv[e];
+    if (di != 0.f) {
+      d32[e] += alpha * p32[e];
+      const float re = r32[e] - alpha * w32[e];
+      r32[e] = re;
+      v[0] += (double)(re * di) * (double)re;
+    }
+  }
+  if (grid_sum<1>(v, partials, &st->counter)) {
+    const double en = v[0];
+    const int m = st->m + 1;
+    st->m = m;
+    bool stop = false;
+    if (m % st->check == 0 && (!isfinite(en) || en < st->thresh_in)) stop = true;
+    if (m >= st->cg_max) stop = true;
+    if (stop) {
+      st->done = 1;
+      st->iters = m;
+    } else {
+      st->beta = en / (st->eta != 0.0 ? st->eta : INFINITY);
+      st->eta = en;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_p32(long long ne, const float* __restrict__ r32,
+                                                     const float* __restrict__ dinv, float* p32,
+                                                     const CGState* st) {
+  if (st->done) return;
+  const float beta = (float)st->beta;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x)
+    p32[e] = r32[e] * dinv[e] + beta * p32[e];
+}
+
+// correction: d64 = d32, x += d64
+__global__ void k_mix_apply(long long ne, const float* __restrict__ d32, double* d64, double* x) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double d = (double)d32[e];
+    d64[e] = d;
+    x[e] += d;
+  }
+}
+
+// r64 -= A d (masked); eta = sum (r*prec)*r with the float64 criterion's preconditioner
+__global__ void __launch_bounds__(kThreads) k_mix_resid(long long ne, double* r64,
+                                                        const double* __restrict__ Ad,
+                                                        const double* __restrict__ prec,
+                                                        double* partials, CGState* st) {
+  double v[2] = {0.0, 0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double pr = prec[e];
+    if (pr == 0.0) continue;
+    const double re = r64[e] - Ad[e];
+    r64[e] = re;
+    v[0] += (re * pr) * re;
+    v[1] += re * re;
+  }
+  if (grid_sum<2>(v, partials, &st->counter)) {
+    st->true_eta = v[0];
+    st->true_l2 = v[1];
+  }
+}
+
+// diagonal probing: p = 1 on the edges of one colour (level L, axis a, index residues mod q)
+__global__ void k_probe_set(long long ne, long long base, int dx, int dy, int cnt, int q, int ci, int cj,
+                            int ck, double* p, int clear) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    const long long loc = e - base;
+    if (loc >= 0 && loc < cnt && !clear) {
+      const int l = (int)loc;
+      const int i = l % dx, j = (l / dx) % dy, k = l / (dx * dy);
+      if (i % q == ci && j % q == cj && k % q == ck) v = 1.0;
+    }
+    p[e] = v;
+  }
+}
+
+__global__ void k_probe_get(long long base, int dx, int dy, int cnt, int q, int ci, int cj, int ck,
+                            const double* __restrict__ w, double* diag) {
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < cnt; l += gridDim.x * blockDim.x) {
+    const int i = l % dx, j = (l / dx) % dy, k = l / (dx * dy);
+    if (i % q == ci && j % q == cj && k % q == ck) diag[base + l] = w[base + l];
+  }
+}
+
+// dinv = 1/(rou*diag1 + kfac*diag2) on unmasked edges, 0 elsewhere
+__global__ void k_dinv(long long ne, const double* __restrict__ d1, const double* __restrict__ d2,
+                       const double* __restrict__ prec, double rou, double kfac, float* dinv) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double d = rou * d1[e] + kfac * d2[e];
+    dinv[e] = (prec[e] != 0.0 && d > 0.0) ? (float)(1.0 / d) : 0.f;
   }
 }
 
@@ -860,7 +1104,7 @@ __global__ void __launch_bounds__(kThreads) k_diag(long long nc, long long ncx, 
   if (threadIdx.x == 0) {
     for (int q = 1; q < (int)(blockDim.x >> 5); ++q) { smax = fmax(smax, sh[0][q]); dmax = fmax(dmax, sh[1][q]); }
     partials[blockIdx.x] = smax;
-    partials[kMaxBlocks + blockIdx.x] = dmax;
+    partials[kPartStride + blockIdx.x] = dmax;
     __threadfence();
     unsigned int t = atomicAdd(&st->counter, 1u);
     if (t == gridDim.x - 1) {
@@ -868,7 +1112,7 @@ __global__ void __launch_bounds__(kThreads) k_diag(long long nc, long long ncx, 
       double a = 0.0, b = 0.0;
       for (int q = 0; q < (int)gridDim.x; ++q) {
         a = fmax(a, ((volatile double*)partials)[q]);
-        b = fmax(b, ((volatile double*)partials)[kMaxBlocks + q]);
+        b = fmax(b, ((volatile double*)partials)[kPartStride + q]);
       }
       out[0] = a; out[1] = b;
       st->counter = 0u;
@@ -988,28 +1232,35 @@ int op_convdiff(pyib_ctx* ctx, int mode, double c1, double c2, double dt, const 
 }
 
 // ---- matvec ---------------------------------------------------------------
-int launch_matvec(pyib_ctx* ctx, const double* in, double* out, int alpd, int do_dot) {
-  const long long nc = ctx->lay.ncell, ne = ctx->lay.nedge;
-  k_mvA<double><<<grid_for(nc), kThreads, 0, ctx->stream>>>(
-      ctx->meta, in, ctx->vcm, tp<unsigned int>(ctx, PYIB_T_PA_BITS), tp<int>(ctx, PYIB_T_PA_ROW),
-      tp<long long>(ctx, PYIB_T_PA_PTR), tp<int>(ctx, PYIB_T_PA_COL), tp<double>(ctx, PYIB_T_PA_VAL),
-      ctx->nA, ctx->st);
+template <typename T>
+int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* pdot, int alpd,
+                    int do_dot, const T* pa_val, const T* pv_val, const T* pr_val) {
+  const Meta& m = ctx->meta;
+  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
+  k_mvA<T><<<gA, blk, 0, ctx->stream>>>(
+      m, in, vcm, tp<unsigned int>(ctx, PYIB_T_PA_BITS), tp<int>(ctx, PYIB_T_PA_ROW),
+      tp<long long>(ctx, PYIB_T_PA_PTR), tp<int>(ctx, PYIB_T_PA_COL), pa_val, ctx->nA, ctx->st);
   CKL();
-  const double* vsrc = ctx->vcm;
+  const T* vsrc = vcm;
   if (alpd) {
-    k_mvV<double><<<grid_for(nc), kThreads, 0, ctx->stream>>>(
-        ctx->meta, ctx->vcm, ctx->vq, tp<unsigned int>(ctx, PYIB_T_PV_BITS), tp<int>(ctx, PYIB_T_PV_ROW),
-        tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL), tp<double>(ctx, PYIB_T_PV_VAL),
-        ctx->st);
+    k_mvV<T><<<gA, blk, 0, ctx->stream>>>(
+        m, vcm, vq, tp<unsigned int>(ctx, PYIB_T_PV_BITS), tp<int>(ctx, PYIB_T_PV_ROW),
+        tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL), pv_val, ctx->st);
     CKL();
-    vsrc = ctx->vq;
+    vsrc = vq;
   }
-  k_mvRI<double><<<grid_for(ne), kThreads, 0, ctx->stream>>>(
-      ctx->meta, vsrc, out, ctx->p, tp<unsigned int>(ctx, PYIB_T_PR_BITS), tp<int>(ctx, PYIB_T_PR_ROW),
-      tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL), tp<double>(ctx, PYIB_T_PR_VAL),
-      ctx->partials, ctx->st, do_dot);
+  k_mvRI<T><<<gR, blk, 0, ctx->stream>>>(
+      m, vsrc, out, pdot, tp<unsigned int>(ctx, PYIB_T_PR_BITS), tp<int>(ctx, PYIB_T_PR_ROW),
+      tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL), pr_val, ctx->partials, ctx->st,
+      do_dot);
   CKL();
   return PYIB_OK;
+}
+
+int launch_matvec(pyib_ctx* ctx, const double* in, double* out, int alpd, int do_dot) {
+  return launch_matvec_t<double>(ctx, in, out, ctx->vcm, ctx->vq, ctx->p, alpd, do_dot,
+                                 tp<double>(ctx, PYIB_T_PA_VAL), tp<double>(ctx, PYIB_T_PV_VAL),
+                                 tp<double>(ctx, PYIB_T_PR_VAL));
 }
 
 int set_state_solver(pyib_ctx* ctx, double dt, int alpd) {
@@ -1139,6 +1390,197 @@ int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   return PYIB_OK;
 }
 
+// ---- mixed precision --------------------------------------------------------
+int set_state_raw(pyib_ctx* ctx, double rou, double kfac) {
+  CGState h{};
+  CK(cudaMemcpyAsync(&h, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  h.rou = rou;
+  h.kfac = kfac;
+  h.done = 0;
+  h.counter = 0u;
+  CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  return PYIB_OK;
+}
+
+int ensure_mixed(pyib_ctx* ctx) {
+  if (ctx->r32) return PYIB_OK;
+  const long long ne = ctx->lay.nedge, nc = ctx->lay.ncell;
+  float** ef[] = {&ctx->r32, &ctx->p32, &ctx->w32, &ctx->x32, &ctx->prec32};
+  for (float** f : ef) RET(alloc(ctx, (void**)f, ne * sizeof(float)));
+  RET(alloc(ctx, (void**)&ctx->vcm32, 3 * nc * sizeof(float)));
+  RET(alloc(ctx, (void**)&ctx->vq32, 3 * nc * sizeof(float)));
+  RET(alloc(ctx, (void**)&ctx->diag1, ne * sizeof(double)));
+  RET(alloc(ctx, (void**)&ctx->diag2, ne * sizeof(double)));
+  const int tabs[3] = {PYIB_T_PA_VAL, PYIB_T_PV_VAL, PYIB_T_PR_VAL};
+  float** outs[3] = {&ctx->pa_val32, &ctx->pv_val32, &ctx->pr_val32};
+  for (int q = 0; q < 3; ++q) {
+    const long long n = (long long)(ctx->tab[tabs[q]].bytes / 8);
+    RET(alloc(ctx, (void**)outs[q], (n > 0 ? n : 1) * sizeof(float)));
+    if (n > 0) {
+      k_d2f<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, tp<double>(ctx, tabs[q]), *outs[q]);
+      CKL();
+    }
+  }
+  return PYIB_OK;
+}
+
+// diag(A) = rou*diag1 + kfac*diag2 by probing with one colour of edges at a time:
+// same level and axis, index residues mod 5 (A couples edges at most 3 apart, so no
+// two edges of one colour share a row entry).
+int build_diag(pyib_ctx* ctx) {
+  if (ctx->diag_ready) return PYIB_OK;
+  const long long ne = ctx->lay.nedge;
+  const int q = 5;
+  double* probe = ctx->work_e;
+  double* out = ctx->w;
+  CK(cudaMemsetAsync(probe, 0, ne * sizeof(double), ctx->stream));
+  for (int pass = 0; pass < 2; ++pass) {
+    RET(set_state_raw(ctx, pass == 0 ? 1.0 : 0.0, pass == 0 ? 0.0 : 1.0));
+    double* dst = pass == 0 ? ctx->diag1 : ctx->diag2;
+    for (int L = 0; L < ctx->meta.nl; ++L) {
+      const LevelMeta& l = ctx->meta.lv[L];
+      for (int a = 0; a < 3; ++a) {
+        const int dx = l.n[0] + (a != 0), dy = l.n[1] + (a != 1);
+        const int cnt = (int)l.ecount[a];
+        const long long base = l.ebase[a];
+        const int g = grid_for(cnt);
+        for (int ci = 0; ci < q; ++ci)
+          for (int cj = 0; cj < q; ++cj)
+            for (int ck = 0; ck < q; ++ck) {
+              k_probe_set<<<g, kThreads, 0, ctx->stream>>>(cnt, 0, dx, dy, cnt, q, ci, cj, ck, probe + base, 0);
+              CKL();
+              RET(launch_matvec(ctx, probe, out, pass, 0));
+              k_probe_get<<<g, kThreads, 0, ctx->stream>>>(base, dx, dy, cnt, q, ci, cj, ck, out, dst);
+              CKL();
+              k_probe_set<<<g, kThreads, 0, ctx->stream>>>(cnt, 0, dx, dy, cnt, q, ci, cj, ck, probe + base, 1);
+              CKL();
+            }
+      }
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->diag_ready = true;
+  return PYIB_OK;
+}
+
+int mix_iteration(pyib_ctx* ctx) {
+  RET(launch_matvec_t<float>(ctx, ctx->p32, ctx->w32, ctx->vcm32, ctx->vq32, ctx->p32, 1, 1,
+                             ctx->pa_val32, ctx->pv_val32, ctx->pr_val32));
+  const long long ne = ctx->lay.nedge;
+  k_cg_update32<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
+                                                            ctx->prec32, ctx->partials, ctx->st);
+  CKL();
+  k_cg_p32<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r32, ctx->prec32, ctx->p32, ctx->st);
+  CKL();
+  return PYIB_OK;
+}
+
+int build_mix_graph(pyib_ctx* ctx) {
+  if (ctx->mix_graph && ctx->mix_graph_check == ctx->prm.check) return PYIB_OK;
+  if (ctx->mix_graph) {
+    cudaGraphExecDestroy(ctx->mix_graph);
+    ctx->mix_graph = nullptr;
+  }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = PYIB_OK;
+  for (int q = 0; q < ctx->prm.check && rc == PYIB_OK; ++q) rc = mix_iteration(ctx);
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc != PYIB_OK) return rc;
+  if (e != cudaSuccess) return set_err(ctx, PYIB_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&ctx->mix_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_err(ctx, PYIB_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+  ctx->mix_graph_check = ctx->prm.check;
+  return PYIB_OK;
+}
+
+int clear_done(pyib_ctx* ctx) {
+  int zero = 0;
+  CK(cudaMemcpyAsync(&ctx->st->done, &zero, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  return PYIB_OK;
+}
+
+// Mixed precision: the float64 stopping test of helm_solve on the true residual,
+// reached by float32 PCG corrections (Jacobi on diag(A)) and float64 residual updates.
+int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
+  const long long ne = ctx->lay.nedge;
+  const double* prec = tp<double>(ctx, PYIB_T_PREC);
+  RET(ensure_mixed(ctx));
+  RET(build_diag(ctx));
+  const double kfac = 0.5 * dt * ctx->prm.visc;
+  if (ctx->diag_for_kfac != kfac || ctx->diag_for_rou != ctx->prm.rou) {
+    k_dinv<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->diag1, ctx->diag2, prec, ctx->prm.rou, kfac,
+                                                      ctx->prec32);
+    CKL();
+    ctx->diag_for_kfac = kfac;
+    ctx->diag_for_rou = ctx->prm.rou;
+  }
+  RET(set_state_solver(ctx, dt, 1));
+  RET(build_mix_graph(ctx));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  k_cg_init<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->res_e, ctx->s, prec, ctx->x, ctx->r,
+                                                        ctx->p, ctx->partials, ctx->st);
+  CKL();
+  CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const double thresh = ctx->st_host->thresh, l2_0 = ctx->st_host->l2_0, eta0 = ctx->st_host->eta;
+  double eta = eta0, l2 = l2_0;
+  int inner_total = 0, sweeps = 0;
+  const double eps2 = ctx->prm.mixed_tol * ctx->prm.mixed_tol;
+  const int max_sweeps = ctx->prm.mixed_max_sweeps > 0 ? ctx->prm.mixed_max_sweeps : 40;
+  while (!(eta < thresh) && sweeps < max_sweeps) {
+    k_mix_start<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
+                                                            ctx->p32, eps2, ctx->partials, ctx->st);
+    CKL();
+    const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
+    for (long long q = 0; q < max_chunks; ++q) {
+      CK(cudaGraphLaunch(ctx->mix_graph, ctx->stream));
+      ctx->launches += 5LL * ctx->prm.check;
+      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (ctx->st_host->done) break;
+    }
+    inner_total += ctx->st_host->iters;
+    k_mix_apply<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, ctx->work_e2, ctx->x);
+    CKL();
+    RET(clear_done(ctx));
+    RET(launch_matvec(ctx, ctx->work_e2, ctx->w, 1, 0));
+    k_mix_resid<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->w, prec, ctx->partials, ctx->st);
+    CKL();
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    eta = ctx->st_host->true_eta;
+    l2 = ctx->st_host->true_l2;
+    ++sweeps;
+    if (!std::isfinite(eta)) break;
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->s, ctx->x, ne * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->cg_seconds += ms * 1e-3;
+  ctx->cg_iters += inner_total;
+  const bool finite = std::isfinite(eta) && std::isfinite(l2) && eta >= 0 && l2 >= 0;
+  pyib_solve_stats st{};
+  st.iterations = inner_total;
+  st.refinements = sweeps;
+  st.rel_residual = finite && l2_0 > 0 ? std::sqrt(l2 / l2_0) : (finite && l2 == 0 ? 0.0 : INFINITY);
+  st.tol_ratio = finite && thresh > 0 ? std::sqrt(eta / thresh) : (finite && eta == 0 ? 0.0 : INFINITY);
+  st.converged = finite && eta <= thresh;
+  st.eta0 = eta0;
+  st.threshold = thresh;
+  if (out) *out = st;
+  if (ctx->prm.strict && !st.converged)
+    return set_err(ctx, PYIB_E_NOCONV,
+                   "mixed-precision Helmholtz solve did not converge: sweeps=%d, inner iterations=%d, "
+                   "mixed_tolerance_ratio=%.6e",
+                   sweeps, inner_total, st.tol_ratio);
+  return PYIB_OK;
+}
+
 // ---- immersed boundary --------------------------------------------------
 int ib_stencil(pyib_ctx* ctx) {
   if (ctx->M <= 0) return set_err(ctx, PYIB_E_STATE, "no markers");
@@ -1238,7 +1680,7 @@ int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* ma
     RET(op_integr(ctx, ctx->res_c, nc, ctx->F));
     RET(op_rot(ctx, ctx->F, ctx->res_e));
     pyib_solve_stats ss{};
-    int rc = helm_solve(ctx, dt, &ss);
+    int rc = ctx->prm.precision == 1 ? helm_solve_mixed(ctx, dt, &ss) : helm_solve(ctx, dt, &ss);
     st.max_iterations = ss.iterations > st.max_iterations ? ss.iterations : st.max_iterations;
     st.total_iterations += ss.iterations;
     st.max_rel_residual = fmax(st.max_rel_residual, ss.rel_residual);
@@ -1322,6 +1764,35 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
     }
   }
   m.nc = cb; m.nf = fb; m.ne = eb;
+  {
+    // z-chunk depth: the deepest of 16, 8, 4, 2, 1 planes that still yields enough tiles
+    long long plane_tiles = 0;
+    for (int L = 0; L < m.nl; ++L) {
+      const LevelMeta& l = m.lv[L];
+      plane_tiles += (long long)((l.n[0] + TX - 1) / TX) * ((l.n[1] + TY - 1) / TY) * l.n[2];
+    }
+    int kz = 16;
+    while (kz > 1 && plane_tiles / kz < kTargetBlocks) kz >>= 1;
+    m.kz = kz;
+    int zA = 0, zR = 0, gxA = 1, gyA = 1, gxR = 1, gyR = 1;
+    for (int L = 0; L < m.nl; ++L) {
+      LevelMeta& l = m.lv[L];
+      l.zbA = zA;
+      l.zbR = zR;
+      zA += (l.n[2] + kz - 1) / kz;
+      zR += (l.n[2] + 1 + kz - 1) / kz;
+      gxA = std::max(gxA, (l.n[0] + TX - 1) / TX);
+      gyA = std::max(gyA, (l.n[1] + TY - 1) / TY);
+      gxR = std::max(gxR, (l.n[0] + TX - 1) / (TX - 1));
+      gyR = std::max(gyR, (l.n[1] + TY - 1) / (TY - 1));
+    }
+    m.gxA = gxA; m.gyA = gyA; m.gzA = zA;
+    m.gxR = gxR; m.gyR = gyR; m.gzR = zR;
+    if ((long long)gxR * gyR * zR > kPartStride || (long long)gxA * gyA * zA > (1LL << 31)) {
+      delete ctx;
+      return PYIB_E_ARG;
+    }
+  }
   if (cb != layout->ncell || fb != layout->nface || eb != layout->nedge) {
     delete ctx;
     return PYIB_E_ARG;
@@ -1345,7 +1816,7 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
     double** c3_fields[] = {&ctx->res_c0, &ctx->res_c, &ctx->fE, &ctx->conv, &ctx->diff, &ctx->work_c3,
                             &ctx->vcm, &ctx->vq};
     for (double** f : c3_fields) RET(alloc(ctx, (void**)f, 3 * nc * sizeof(double)));
-    RET(alloc(ctx, (void**)&ctx->partials, kSlots * kMaxBlocks * sizeof(double)));
+    RET(alloc(ctx, (void**)&ctx->partials, (size_t)kSlots * kPartStride * sizeof(double)));
     RET(alloc(ctx, (void**)&ctx->st, sizeof(CGState)));
     CK(cudaMallocHost((void**)&ctx->st_host, sizeof(CGState)));
     RET(alloc(ctx, (void**)&ctx->dev_err, sizeof(int)));
@@ -1366,6 +1837,7 @@ int pyib_destroy(pyib_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->cg_graph) cudaGraphExecDestroy(ctx->cg_graph);
+  if (ctx->mix_graph) cudaGraphExecDestroy(ctx->mix_graph);
   for (auto& t : ctx->tab)
     if (t.ptr) cudaFree(t.ptr);
   void* ptrs[] = {ctx->s, ctx->s_old, ctx->U, ctx->vc, ctx->res_c0, ctx->res_c, ctx->res_e, ctx->F,
@@ -1374,7 +1846,8 @@ int pyib_destroy(pyib_ctx* ctx) {
                   ctx->dev_err, ctx->mk, ctx->mvel, ctx->ds, ctx->fL, ctx->lag, ctx->dL, ctx->ibw,
                   ctx->ibcell, ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
                   ctx->sort_vals_out, ctx->sort_tmp, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
-                  ctx->vcm32, ctx->vq32, ctx->prec32};
+                  ctx->vcm32, ctx->vq32, ctx->prec32, ctx->pa_val32, ctx->pv_val32,
+                  ctx->pr_val32, ctx->diag1, ctx->diag2};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
@@ -1402,11 +1875,23 @@ int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes) {
   t.bytes = bytes;
   if (bytes) CK(cudaMemcpyAsync(t.ptr, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (table == PYIB_T_PA_VAL || table == PYIB_T_PV_VAL || table == PYIB_T_PR_VAL) {
+    float** f = table == PYIB_T_PA_VAL ? &ctx->pa_val32 : (table == PYIB_T_PV_VAL ? &ctx->pv_val32 : &ctx->pr_val32);
+    if (*f) { cudaFree(*f); *f = nullptr; }
+    if (ctx->r32) {
+      const long long n = (long long)(bytes / 8);
+      RET(alloc(ctx, (void**)f, (n > 0 ? n : 1) * sizeof(float)));
+      if (n > 0) { k_d2f<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, (const double*)t.ptr, *f); CKL(); }
+    }
+  }
   if (table == PYIB_T_INLET_IDX) ctx->n_inlet = bytes / 4;
   if (table == PYIB_T_BF_FACE) ctx->n_bf = bytes / 4;
   if (table == PYIB_T_LC_CAND) ctx->n_cand = bytes / 4;
   if (table == PYIB_T_LC_FIDX) ctx->n_fidx = bytes / 4;
   ctx->cg_graph_check = -1;  // tables changed: recapture
+  ctx->mix_graph_check = -1;
+  ctx->diag_ready = false;
+  ctx->diag_for_kfac = -1.0;
   return PYIB_OK;
 }
 
@@ -1429,7 +1914,11 @@ int pyib_set_params(pyib_ctx* ctx, const pyib_params* p) {
   const bool recapture = !ctx->have_params || ctx->prm.check != p->check;
   ctx->prm = *p;
   ctx->have_params = true;
-  if (recapture) ctx->cg_graph_check = -1;
+  if (recapture) {
+    ctx->cg_graph_check = -1;
+    ctx->mix_graph_check = -1;
+  }
+  if (p->precision != 0 && p->precision != 1) return set_err(ctx, PYIB_E_ARG, "precision must be 0 or 1");
   if (p->nmarkers > 0) RET(ib_alloc(ctx, p->nmarkers));
   return PYIB_OK;
 }
@@ -1469,6 +1958,7 @@ static int field_ptr(pyib_ctx* ctx, int32_t f, void** ptr, size_t* count, size_t
     case PYIB_F_IB_W: *ptr = ctx->ibw; *count = 125 * M; *writable = false; break;
     case PYIB_F_IB_BASE: *ptr = ctx->ibbase; *count = 3 * M; *elem = 4; *writable = false; break;
     case PYIB_F_LAG_TMP: *ptr = ctx->lag; *count = 3 * M; break;
+    case PYIB_F_DINV: *ptr = ctx->prec32; *count = ne; *elem = 4; *writable = false; break;
     default: return set_err(ctx, PYIB_E_ARG, "unknown field %d", f);
   }
   if (!*ptr) return set_err(ctx, PYIB_E_STATE, "field %d is not allocated", f);
@@ -1546,7 +2036,7 @@ int pyib_conv_diff(pyib_ctx* ctx) {
 int pyib_helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* stats) {
   if (!ctx) return PYIB_E_ARG;
   if (!tables_ready(ctx) || !ctx->have_params) return set_err(ctx, PYIB_E_STATE, "context not ready");
-  return helm_solve(ctx, dt, stats);
+  return ctx->prm.precision == 1 ? helm_solve_mixed(ctx, dt, stats) : helm_solve(ctx, dt, stats);
 }
 
 int pyib_step(pyib_ctx* ctx, double dt, double dt_old, int32_t inner, const double* markers,
@@ -1587,7 +2077,7 @@ int pyib_loads(pyib_ctx* ctx, const double* centre, double radius, double width,
   if (!ctx->tab[PYIB_T_LC_CAND].ptr || !ctx->tab[PYIB_T_LC_FIDX].ptr || !ctx->tab[PYIB_T_LC_CPOS].ptr)
     return set_err(ctx, PYIB_E_STATE, "load-correction tables missing");
   const double* c = fixed_centre ? centre0 : centre;
-  double* dout = ctx->partials + (kSlots - 1) * kMaxBlocks;   // 13 doubles of scratch
+  double* dout = ctx->partials + (size_t)(kSlots - 1) * kPartStride;   // 13 doubles of scratch
   const long long n = ctx->n_cand > ctx->n_fidx ? ctx->n_cand : ctx->n_fidx;
   k_loads<<<grid_for(n), kThreads, 0, ctx->stream>>>(
       ctx->n_cand, tp<int>(ctx, PYIB_T_LC_CAND), ctx->n_fidx, tp<int>(ctx, PYIB_T_LC_FIDX),
@@ -1605,7 +2095,7 @@ int pyib_loads(pyib_ctx* ctx, const double* centre, double radius, double width,
 
 int pyib_diagnostics(pyib_ctx* ctx, double* out) {
   if (!ctx || !out) return PYIB_E_ARG;
-  double* dout = ctx->partials + (kSlots - 1) * kMaxBlocks;
+  double* dout = ctx->partials + (size_t)(kSlots - 1) * kPartStride;
   k_diag<<<grid_for(ctx->lay.ncell), kThreads, 0, ctx->stream>>>(
       ctx->lay.ncell, ncx_of(ctx), ctx->vc, tp<long long>(ctx, PYIB_T_CF_PTR), tp<int>(ctx, PYIB_T_CF_FACE),
       tp<double>(ctx, PYIB_T_VOLCI), ctx->U, ctx->partials, ctx->st, dout);

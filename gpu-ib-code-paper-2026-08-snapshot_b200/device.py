@@ -58,7 +58,7 @@ class DeviceSolver:
 
     def __init__(self, lay: NestedLayout, *, rou, visc, cavity, cg_check_interval=20,
                  cg_max_iterations=1000, strict=False, ac=0.5, ad=0.5, tol1=1e-10, tol2=1e-9,
-                 device=0):
+                 device=0, precision="float64", mixed_tol=1e-4, mixed_max_sweeps=40):
         if not getattr(lay, "_built", False):
             lay.build()
         self.lay = lay
@@ -87,8 +87,10 @@ class DeviceSolver:
         self._upload_tables()
         self.params = dict(rou=float(rou), visc=float(visc), ac=ac, ad=ad, tol1=tol1, tol2=tol2,
                            cavity=int(self.cavity), check=int(cg_check_interval),
-                           cg_max=int(cg_max_iterations), strict=int(bool(strict)), precision=0,
-                           nmarkers=0, hh=lay.h0, hh3=lay.h0 ** 3)
+                           cg_max=int(cg_max_iterations), strict=int(bool(strict)),
+                           precision={"float64": 0, "mixed": 1}[precision],
+                           nmarkers=0, hh=lay.h0, hh3=lay.h0 ** 3, mixed_tol=float(mixed_tol),
+                           mixed_max_sweeps=int(mixed_max_sweeps))
         self._push_params()
         pos_ref = (lay.levels[0].lo + 0.5 * lay.h0).astype(np.float64)
         self.pos_ref = pos_ref
@@ -207,6 +209,10 @@ class DeviceSolver:
 
     def set(self, name, arr):
         self.h.set_field(name, arr)
+
+    def get_dinv(self):
+        """The mixed solver's float32 Jacobi preconditioner 1/diag(A) (0 on masked edges)."""
+        return self.h.get_field("DINV", self.lay.NE, np.float32).astype(np.float64)
 
     def vc_cells(self):
         """Cell velocity (3, NC) without ghosts."""

@@ -47,7 +47,12 @@ class B200Driver:
     fail_on_cg_nonconvergence = False
 
     def __init__(self, layout: NestedLayout, visc, rou=1.0, ac=0.5, ad=0.5, *,
-                 cg_max_iterations=1000, fail_on_cg_nonconvergence=False, device=0):
+                 cg_max_iterations=1000, fail_on_cg_nonconvergence=False, device=0,
+                 precision="float64", mixed_tol=1e-4):
+        if precision not in ("float64", "mixed"):
+            raise ValueError("precision must be 'float64' or 'mixed'")
+        self.precision = precision
+        self.mixed_tol = float(mixed_tol)
         if isinstance(cg_max_iterations, bool) or int(cg_max_iterations) <= 0:
             raise ValueError("cg_max_iterations must be a positive integer")
         if not isinstance(fail_on_cg_nonconvergence, (bool, np.bool_)):
@@ -112,7 +117,8 @@ class B200Driver:
                                         cg_check_interval=self.cg_check_interval,
                                         cg_max_iterations=self.cg_max_iterations,
                                         strict=self.fail_on_cg_nonconvergence, ac=self.ac, ad=self.ad,
-                                        device=self.device)
+                                        device=self.device, precision=self.precision,
+                                        mixed_tol=self.mixed_tol)
             self._ib_dirty = True
         sv = self._solver
         want = dict(check=int(self.cg_check_interval), cg_max=int(self.cg_max_iterations),

@@ -70,6 +70,10 @@ typedef struct pyib_params {
   int32_t nmarkers;          /* Lagrangian markers                              */
   double hh;                 /* delta-kernel width (ImmersedBoundary.hh)        */
   double hh3;                /* hh**3 as the host computes it (ib_immersed.py:89) */
+  double mixed_tol;          /* precision 1: inner float32 solve reduces the
+                                preconditioned residual norm by this factor      */
+  int32_t mixed_max_sweeps;  /* precision 1: cap on float64 refinement sweeps   */
+  int32_t pad;
 } pyib_params;
 
 /* Per-solve statistics (Driver.helm_solve finish(), ib_driver_np.py:338-377). */
@@ -135,6 +139,7 @@ enum pyib_field {
   PYIB_F_IB_W,         /* f64[125*M] stencil weights, read only               */
   PYIB_F_IB_BASE,      /* i32[3*M] rint((x - pos_ref)/dx), read only          */
   PYIB_F_LAG_TMP,      /* f64[3*M] last interpolated marker velocity          */
+  PYIB_F_DINV,         /* f32[nedge] mixed solver's 1/diag(A), read only      */
   PYIB_F_COUNT
 };
 
