@@ -2175,3 +2175,64 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Spreading without allocation.
+//
+// Some callers cannot call cudaMalloc: a coupling code that runs inside a
+// memory budget fixed at start-up, or a host framework whose allocator owns
+// all device memory, still needs the deterministic spreading of Lagrangian
+// forces.  pyib_spread_noalloc keeps all its scratch (sort keys and values in
+// two ping-pong pairs, and CUB's temporary storage) in one file-scope
+// __device__ array of fixed size; every GPU that loads this library holds it
+// until the process exits.  The caller passes inputs and the output.
+// ===========================================================================
+namespace {
+constexpr long long kNoAllocMaxMarkers = 8192;                      // 1,024,000 contributions
+constexpr long long kNoAllocMaxItems = kNoAllocMaxMarkers * 125;
+constexpr size_t kNoAllocSortBytes = 4ull * kNoAllocMaxItems * sizeof(int);   // 16,384,000
+constexpr size_t kNoAllocTempBytes = 1ull << 20;                   // CUB histograms and offsets
+constexpr size_t kNoAllocBytes = kNoAllocSortBytes + kNoAllocTempBytes;
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_spread_scratch[kNoAllocBytes];
+static void* g_spread_scratch_ptr[kNoAllocMaxDevices] = {nullptr};
+
+extern "C" int pyib_spread_noalloc(const int32_t* cell, const double* w, const double* ds3, const double* f,
+                                   int32_t nmarkers, int64_t ncell, double* out, void* stream) {
+  if (!cell || !w || !ds3 || !f || !out) return PYIB_E_ARG;
+  if (nmarkers <= 0 || nmarkers > kNoAllocMaxMarkers) return PYIB_E_ARG;
+  if (ncell <= 0 || ncell >= (1LL << 31)) return PYIB_E_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PYIB_E_CUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return PYIB_E_ARG;
+  if (!g_spread_scratch_ptr[dev]) {
+    // Host code only sees a stand-in for the array; the kernels need its device address.
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_spread_scratch) != cudaSuccess || !p) return PYIB_E_CUDA;
+    g_spread_scratch_ptr[dev] = p;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long tot = (long long)nmarkers * 125;
+  int* keys_a = (int*)g_spread_scratch_ptr[dev];
+  int* keys_b = keys_a + kNoAllocMaxItems;
+  int* vals_a = keys_b + kNoAllocMaxItems;
+  int* vals_b = vals_a + kNoAllocMaxItems;
+  void* temp = (void*)((unsigned char*)g_spread_scratch_ptr[dev] + kNoAllocSortBytes);
+  int nbits = 1;
+  while (nbits < 31 && (1LL << nbits) < ncell) ++nbits;
+  cub::DoubleBuffer<int> dk(keys_a, keys_b), dv(vals_a, vals_b);
+  size_t tb = 0;
+  if (cub::DeviceRadixSort::SortPairs((void*)nullptr, tb, dk, dv, (int)tot, 0, nbits, s) != cudaSuccess)
+    return PYIB_E_CUDA;
+  if (tb > kNoAllocTempBytes) return PYIB_E_ARG;
+  if (cudaMemsetAsync(out, 0, 3 * (size_t)ncell * sizeof(double), s) != cudaSuccess) return PYIB_E_CUDA;
+  k_ib_keys<<<grid_for(tot), kThreads, 0, s>>>(tot, cell, w, dk.Current(), dv.Current());
+  if (cudaGetLastError() != cudaSuccess) return PYIB_E_CUDA;
+  if (cub::DeviceRadixSort::SortPairs(temp, tb, dk, dv, (int)tot, 0, nbits, s) != cudaSuccess)
+    return PYIB_E_CUDA;
+  k_ib_segsum<<<grid_for(tot), kThreads, 0, s>>>(tot, ncell, dk.Current(), dv.Current(), w, ds3, f, out);
+  if (cudaGetLastError() != cudaSuccess) return PYIB_E_CUDA;
+  return PYIB_OK;
+}

@@ -218,6 +218,28 @@ int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms);
  * events; *ms_per = milliseconds per matvec (benchmark support). */
 int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
 
+/* Deterministic spreading that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc (a code running inside a device-memory
+ * budget fixed at start-up, or one whose framework allocator owns all device
+ * memory).  Same result as pyib_ib_spread: out[d*ncell + c] = sum over the
+ * contributions with cell c, in (marker, offset) order, of f[3*m+d] * w * ds3[m].
+ * All pointers are device pointers: cell/w are the 125*nmarkers stencil cells and
+ * weights (PYIB_F_IB_CELL, PYIB_F_IB_W), ds3 the marker volumes, f the marker-major
+ * forces, out 3*ncell doubles (component-major, fully overwritten).
+ *  - Scratch: one fixed file-scope device array of 17,408,000 bytes, enough for at
+ *    most 8192 markers; larger counts return PYIB_E_ARG.  Every GPU that loads the
+ *    library holds this array until the process exits.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call before
+ *    any stream capture.
+ *  - Calls share the array: calls that overlap on the GPU (different streams, or
+ *    threads without ordering) race.  Run them in one stream or serialize them.
+ *  - stream is a cudaStream_t (NULL: the legacy default stream).  The call is
+ *    asynchronous with respect to the host. */
+int pyib_spread_noalloc(const int32_t* cell, const double* w, const double* ds3, const double* f,
+                        int32_t nmarkers, int64_t ncell, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
