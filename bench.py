@@ -288,7 +288,7 @@ def run_b200(args, world, rank, local):
     barrier(dist)
     sampler = ClockSampler(local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
     sampler.start()
-    timing = (C.c_double * 3)()
+    timing = (C.c_double * 5)()
     sv.h.call("pyib_cg_timing", timing, 1)
     iters = []
     ev_ms = C.c_double(0.0)
@@ -303,6 +303,7 @@ def run_b200(args, world, rank, local):
     sv.h.call("pyib_event", 1, C.byref(ev_ms))
     sv.h.call("pyib_cg_timing", timing, 1)
     cg_s, cg_it, launches = float(timing[0]), float(timing[1]), int(timing[2])
+    tiles = {"cell_tile": [32, 8, int(timing[3])], "node_tile": [32, 8, int(timing[4])]}
     t_dev = ev_ms.value / 1000.0
     barrier(dist)
     # e2e: public API, host inputs and a host read of the step's load every step
@@ -359,6 +360,7 @@ def run_b200(args, world, rank, local):
             "cg": {"seconds": cg_s, "iterations": cg_it, "ms_per_iteration": 1e3 * t_iter,
                    "gbs": achieved},
             "gpu_launches": launches,
+            "autotuned_tiles": tiles,
             "clocks": clocks,
         }
         if cpu is not None:

@@ -1,0 +1,514 @@
+"""JSON case runner for the B200 path: config, runtime assembly, step loop, history, checkpoints.
+
+The configuration is the reference's schema v1 (``ib_case.py:56-110``) with one
+added device value, ``runtime.device = "b200"``, and the precisions
+``"float64"`` (the reference's arithmetic) and ``"mixed"`` (float32 PCG inside
+float64 refinement).  Mesh kinds follow the reference (``uniform_box``,
+``sphere_concentric``, ``sphere_wake``) plus ``nested_boxes`` (concentric cubes
+with explicit half widths in diameters), which the benchmark configurations
+use.  The loop mirrors ``ib_case.run_case`` (``ib_case.py:1413-1648``): the
+clock is anchored to the integer step, sampled steps write a ``history.csv``
+row, checkpoints are atomic NPZ files written after the history is durable,
+SIGTERM/SIGINT/SIGUSR1 stop after the current step with a checkpoint, and a
+resume validates the configuration fingerprint before restoring the state.
+"""
+from __future__ import annotations
+
+import copy
+import csv
+import hashlib
+import json
+import math
+import os
+import signal
+import time
+import uuid
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+from .cases import Oscillation, fibonacci_sphere
+from .driver import B200Driver
+from .layout import NestedLayout
+from .runner import SphereLoads
+
+SCHEMA_VERSION = 1
+CHECKPOINT_SCHEMA_VERSION = 1
+
+DEFAULT_CONFIG: dict[str, Any] = {
+    "schema_version": SCHEMA_VERSION,
+    "name": "fixed_sphere",
+    "case": {"kind": "fixed_sphere"},
+    "runtime": {"device": "b200", "precision": "float64"},
+    "mesh": {"kind": "uniform_box", "dx": 0.25, "bounds": [[-1.0, 1.0], [-1.0, 1.0], [-1.0, 1.0]],
+             "verbose": False},
+    "physics": {"reynolds": 100.0, "density": 1.0, "inflow_speed": 1.0},
+    "time": {"dt": 0.01, "steps": 5, "inner_iterations": 4},
+    "ib": {"radius": 0.25, "center": [0.0, 0.0, 0.0], "marker_spacing": 0.25,
+           "force_mode": "accumulated_explicit", "implicit": False, "alpha": 1.0,
+           "motion": {"kind": "none", "axis": [0.0, 1.0, 0.0], "amplitude": 0.0, "frequency": 1.0,
+                      "phase": 0.0}},
+    "solver": {"sparse": True, "cg_check_interval": 20, "cg_max_iterations": 1000,
+               "fail_on_cg_nonconvergence": False},
+    "output": {"sample_every": 10, "checkpoint_every": 1000, "field_every": 0, "field_start_step": 0,
+               "save_field": True},
+}
+
+_ALLOWED = {
+    "root": {"schema_version", "name", "case", "runtime", "mesh", "physics", "time", "ib", "solver", "output"},
+    "case": {"kind"},
+    "runtime": {"device", "precision", "mixed_tolerance"},
+    "mesh": {"kind", "dx", "bounds", "cells_per_diameter", "half_widths_d", "verbose"},
+    "physics": {"reynolds", "density", "inflow_speed"},
+    "time": {"dt", "steps", "inner_iterations"},
+    "ib": {"radius", "center", "marker_spacing", "force_mode", "implicit", "alpha", "motion"},
+    "motion": {"kind", "axis", "amplitude", "frequency", "phase", "spin_ratio"},
+    "solver": {"sparse", "cg_check_interval", "cg_max_iterations", "fail_on_cg_nonconvergence"},
+    "output": {"sample_every", "checkpoint_every", "field_every", "field_start_step", "save_field"},
+}
+
+# Reference presets (solver/sphere_quiescent_mesh.py:41, solver/sphere_wake_mesh.py:46-51)
+CONCENTRIC_HALF_WIDTHS_D = (1.0, 2.0, 4.0, 8.0, 16.0)
+WAKE_BOUNDS_D = ((-1.0, 3.0, -1.0, 1.0, -1.0, 1.0), (-2.0, 6.0, -2.0, 2.0, -2.0, 2.0),
+                 (-4.0, 12.0, -4.0, 4.0, -4.0, 4.0), (-8.0, 16.0, -8.0, 8.0, -8.0, 8.0))
+
+HISTORY_COLUMNS = [
+    "step", "time", "Cd", "Cy", "Cz", "body_force_x", "body_force_y", "body_force_z",
+    "force_fluid_x", "force_fluid_y", "force_fluid_z", "body_moment_x", "body_moment_y",
+    "body_moment_z", "moment_fluid_x", "moment_fluid_y", "moment_fluid_z",
+    "interior_momentum_x", "interior_momentum_y", "interior_momentum_z",
+    "interior_indicator_volume", "slip_max", "slip_rms", "speed_max", "cfl", "mass_residual_inf",
+    "force_balance_relerr", "ib_force_updates", "helmholtz_iterations",
+    "helmholtz_relative_residual", "helmholtz_tolerance_ratio", "milliseconds_per_step",
+]
+
+
+class CaseConfigError(ValueError):
+    """Invalid case configuration (the reference's ``CaseConfigError``)."""
+
+
+def _merge(base, over):
+    out = copy.deepcopy(base)
+    for k, v in over.items():
+        if isinstance(v, dict) and isinstance(out.get(k), dict):
+            out[k] = _merge(out[k], v)
+        else:
+            out[k] = copy.deepcopy(v)
+    return out
+
+
+def _reject_unknown(section, d):
+    extra = set(d) - _ALLOWED[section]
+    if extra:
+        raise CaseConfigError(f"unknown key(s) in {section}: {sorted(extra)}")
+
+
+def _positive(name, v):
+    try:
+        x = float(v)
+    except (TypeError, ValueError):
+        raise CaseConfigError(f"{name} must be a number") from None
+    if isinstance(v, bool) or not math.isfinite(x) or x <= 0.0:
+        raise CaseConfigError(f"{name} must be finite and positive")
+    return x
+
+
+def _positive_int(name, v):
+    if isinstance(v, bool) or not isinstance(v, (int, np.integer)) or int(v) <= 0:
+        raise CaseConfigError(f"{name} must be a positive integer")
+    return int(v)
+
+
+def validate_config(raw: dict) -> dict:
+    """Merge defaults, reject typos and return a normalized configuration (ib_case.py:262-441)."""
+    if not isinstance(raw, dict):
+        raise CaseConfigError("the case file must contain a JSON object")
+    _reject_unknown("root", raw)
+    for sec in ("case", "runtime", "mesh", "physics", "time", "ib", "solver", "output"):
+        if sec in raw:
+            if not isinstance(raw[sec], dict):
+                raise CaseConfigError(f"{sec} must be a JSON object")
+            _reject_unknown(sec, raw[sec])
+    if isinstance(raw.get("ib"), dict) and isinstance(raw["ib"].get("motion"), dict):
+        _reject_unknown("motion", raw["ib"]["motion"])
+    cfg = _merge(DEFAULT_CONFIG, raw)
+    if cfg["schema_version"] != SCHEMA_VERSION or isinstance(cfg["schema_version"], bool):
+        raise CaseConfigError(f"unsupported schema_version={cfg['schema_version']}; expected {SCHEMA_VERSION}")
+    if not isinstance(cfg["name"], str) or not cfg["name"].strip():
+        raise CaseConfigError("name must be a non-empty string")
+    kind = str(cfg["case"]["kind"])
+    if kind not in {"fixed_sphere", "oscillating_sphere", "rotating_sphere"}:
+        raise CaseConfigError(f"unsupported case.kind={kind!r}")
+    rt = cfg["runtime"]
+    if rt["device"] != "b200":
+        raise CaseConfigError("runtime.device must be 'b200' here ('cpu'/'cuda' are the reference's backends)")
+    if rt["precision"] not in {"float64", "mixed"}:
+        raise CaseConfigError("runtime.precision must be 'float64' or 'mixed'")
+    rt["mixed_tolerance"] = _positive("runtime.mixed_tolerance", rt.get("mixed_tolerance", 1e-4))
+    mesh = cfg["mesh"]
+    mk = str(mesh["kind"])
+    if mk not in {"uniform_box", "sphere_concentric", "sphere_wake", "nested_boxes"}:
+        raise CaseConfigError(f"unsupported mesh.kind={mk!r}")
+    if mk == "uniform_box":
+        mesh["dx"] = _positive("mesh.dx", mesh["dx"])
+        b = np.asarray(mesh["bounds"], dtype=float)
+        if b.shape != (3, 2) or not np.all(np.isfinite(b)) or np.any(b[:, 1] <= b[:, 0]):
+            raise CaseConfigError("mesh.bounds must be three finite [lower, upper] pairs")
+        cells = (b[:, 1] - b[:, 0]) / mesh["dx"]
+        if not np.allclose(cells, np.rint(cells), rtol=0.0, atol=1e-10):
+            raise CaseConfigError("uniform-box side lengths must be integer multiples of mesh.dx")
+        mesh["bounds"] = b.tolist()
+    else:
+        mesh["cells_per_diameter"] = _positive_int("mesh.cells_per_diameter", mesh.get("cells_per_diameter", 16))
+        if mk != "nested_boxes" and mesh["cells_per_diameter"] % 8:
+            raise CaseConfigError("nested-sphere cells_per_diameter must be a multiple of 8")
+        if mk == "nested_boxes":
+            hw = mesh.get("half_widths_d")
+            if not isinstance(hw, list) or not hw or any(_positive("mesh.half_widths_d", x) <= 0 for x in hw):
+                raise CaseConfigError("nested_boxes needs mesh.half_widths_d (innermost first)")
+            mesh["half_widths_d"] = [float(x) for x in hw]
+        mesh.pop("dx", None)
+        mesh.pop("bounds", None)
+    ph = cfg["physics"]
+    ph["reynolds"] = _positive("physics.reynolds", ph["reynolds"])
+    ph["density"] = _positive("physics.density", ph["density"])
+    ph["inflow_speed"] = float(ph["inflow_speed"])
+    tm = cfg["time"]
+    tm["dt"] = _positive("time.dt", tm["dt"])
+    tm["steps"] = _positive_int("time.steps", tm["steps"])
+    tm["inner_iterations"] = _positive_int("time.inner_iterations", tm["inner_iterations"])
+    ib = cfg["ib"]
+    ib["radius"] = _positive("ib.radius", ib["radius"])
+    ib["marker_spacing"] = _positive("ib.marker_spacing", ib["marker_spacing"])
+    if ib["force_mode"] != "accumulated_explicit" or ib["implicit"] or float(ib["alpha"]) != 1.0:
+        raise CaseConfigError("the b200 device runs accumulated_explicit forcing with alpha=1, explicit")
+    if tm["inner_iterations"] < 2:
+        raise CaseConfigError("accumulated_explicit requires at least two fluid inner iterations")
+    mo = ib["motion"]
+    expected = {"fixed_sphere": "none", "oscillating_sphere": "oscillation", "rotating_sphere": "rotation"}[kind]
+    if mo["kind"] != expected:
+        raise CaseConfigError(f"case.kind={kind!r} requires ib.motion.kind={expected!r}")
+    ax = np.asarray(mo["axis"], dtype=float)
+    if ax.shape != (3,) or not np.all(np.isfinite(ax)) or np.linalg.norm(ax) == 0.0:
+        raise CaseConfigError("ib.motion.axis must be a finite non-zero vector")
+    mo["axis"] = (ax / np.linalg.norm(ax)).tolist()
+    mo["amplitude"] = float(mo["amplitude"])
+    mo["frequency"] = _positive("ib.motion.frequency", mo["frequency"])
+    mo["phase"] = float(mo["phase"])
+    if kind == "oscillating_sphere" and mo["amplitude"] <= 0.0:
+        raise CaseConfigError("oscillating_sphere requires a positive motion amplitude")
+    if kind != "oscillating_sphere" and mo["amplitude"] != 0.0:
+        raise CaseConfigError(f"{kind} requires zero translational amplitude")
+    if kind == "rotating_sphere":
+        if "spin_ratio" not in mo:
+            raise CaseConfigError("rotating_sphere requires ib.motion.spin_ratio")
+        mo["spin_ratio"] = float(mo["spin_ratio"])
+    if kind in {"fixed_sphere", "rotating_sphere"} and ph["inflow_speed"] == 0.0:
+        raise CaseConfigError(f"{kind} requires non-zero physics.inflow_speed")
+    so = cfg["solver"]
+    so["cg_check_interval"] = _positive_int("solver.cg_check_interval", so["cg_check_interval"])
+    so["cg_max_iterations"] = _positive_int("solver.cg_max_iterations", so["cg_max_iterations"])
+    if not isinstance(so["fail_on_cg_nonconvergence"], bool):
+        raise CaseConfigError("solver.fail_on_cg_nonconvergence must be true or false")
+    out = cfg["output"]
+    out["sample_every"] = _positive_int("output.sample_every", out["sample_every"])
+    out["checkpoint_every"] = int(out["checkpoint_every"])
+    if mk in {"sphere_wake", "sphere_concentric", "nested_boxes"}:
+        if not np.allclose(ib["center"], 0.0) or not np.isclose(ib["radius"], 0.25):
+            raise CaseConfigError("nested sphere meshes require ib.center=[0,0,0] and ib.radius=0.25")
+    return cfg
+
+
+def config_fingerprint(cfg: dict) -> str:
+    stable = copy.deepcopy(cfg)
+    for k in ("name", "output"):
+        stable.pop(k, None)
+    stable["time"].pop("steps", None)
+    return hashlib.sha256(json.dumps(stable, sort_keys=True, separators=(",", ":")).encode()).hexdigest()
+
+
+def build_layout(cfg):
+    """The nested box list of the configured mesh (make_nested_mesh inputs)."""
+    mesh = cfg["mesh"]
+    D = 2.0 * float(cfg["ib"]["radius"])
+    if mesh["kind"] == "uniform_box":
+        b = np.asarray(mesh["bounds"], float)
+        return NestedLayout(mesh["dx"], [(b[:, 0], b[:, 1])]), float(mesh["dx"]), b
+    h = D / mesh["cells_per_diameter"]
+    if mesh["kind"] == "sphere_wake":
+        boxes = [((bd[0] * D, bd[2] * D, bd[4] * D), (bd[1] * D, bd[3] * D, bd[5] * D)) for bd in WAKE_BOUNDS_D]
+    else:
+        hws = CONCENTRIC_HALF_WIDTHS_D if mesh["kind"] == "sphere_concentric" else mesh["half_widths_d"]
+        boxes = [((-w * D,) * 3, (w * D,) * 3) for w in hws]
+    lo, hi = np.asarray(boxes[0][0]), np.asarray(boxes[0][1])
+    return NestedLayout(h, boxes), h, np.stack([lo, hi], axis=1)
+
+
+@dataclass
+class CaseRuntime:
+    config: dict
+    layout: NestedLayout
+    driver: B200Driver
+    loads: SphereLoads
+    motion: Any
+    dx: float
+    dt: float
+    steps: int
+    inner: int
+    reference_force: float
+    reference_speed: float
+    fingerprint: str
+
+
+def build_runtime(cfg) -> CaseRuntime:
+    """Assemble the B200 runtime as ib_case.build_runtime does (ib_case.py:633-809)."""
+    cfg = validate_config(cfg)
+    lay, dx, fine_bounds = build_layout(cfg)
+    ib = cfg["ib"]
+    radius = float(ib["radius"])
+    centre = np.asarray(ib["center"], float)
+    mo = ib["motion"]
+    exc = np.abs(np.asarray(mo["axis"])) * mo["amplitude"] if mo["kind"] == "oscillation" else np.zeros(3)
+    if np.any(centre - exc - radius - 2.5 * dx < fine_bounds[:, 0] - 1e-12) or \
+            np.any(centre + exc + radius + 2.5 * dx > fine_bounds[:, 1] + 1e-12):
+        raise CaseConfigError("the sphere or its IB support leaves the finest uniform mesh region")
+    ph = cfg["physics"]
+    rho = ph["density"]
+    Dref = 2.0 * radius
+    if ph["inflow_speed"] != 0.0:
+        uref = abs(ph["inflow_speed"])
+    else:
+        uref = 2.0 * np.pi * mo["frequency"] * mo["amplitude"]
+    nu = uref * Dref / ph["reynolds"]
+    so = cfg["solver"]
+    drv = B200Driver(lay, visc=rho * nu, rou=rho, cg_max_iterations=so["cg_max_iterations"],
+                     fail_on_cg_nonconvergence=so["fail_on_cg_nonconvergence"],
+                     precision=cfg["runtime"]["precision"], mixed_tol=cfg["runtime"]["mixed_tolerance"])
+    drv.cg_check_interval = so["cg_check_interval"]
+    if cfg["mesh"]["kind"] in {"sphere_concentric", "nested_boxes"}:
+        drv.set_cavity(U_lid=0.0, spanwise_zerograd=False)
+    count = max(12, int(round(4.0 * np.pi * radius ** 2 / ib["marker_spacing"] ** 2)))
+    markers = fibonacci_sphere(count, radius, centre)
+    width = (4.0 * np.pi * radius ** 2 * dx / count) ** (1.0 / 3.0)
+    ds = np.full(count, width)
+    motion = None
+    if mo["kind"] == "oscillation":
+        motion = Oscillation(markers, mo["axis"], mo["amplitude"], mo["frequency"], mo["phase"])
+        mk0, v0 = motion(0.0)
+        drv.set_ib(None, mk0, ds, v0)
+        drv.set_motion(motion, 0.0)
+    elif mo["kind"] == "rotation":
+        omega = np.asarray(mo["axis"]) * mo["spin_ratio"] * uref / radius
+        drv.set_ib(None, markers, ds, np.cross(omega, markers - centre))
+    else:
+        drv.set_ib(None, markers, ds, np.zeros_like(markers))
+    loads = SphereLoads(drv, centre, exc, radius, dx, rho, 1.5 * dx)
+    return CaseRuntime(config=cfg, layout=lay, driver=drv, loads=loads, motion=motion, dx=dx,
+                       dt=cfg["time"]["dt"], steps=cfg["time"]["steps"],
+                       inner=cfg["time"]["inner_iterations"],
+                       reference_force=0.5 * rho * uref ** 2 * np.pi * radius ** 2, reference_speed=uref,
+                       fingerprint=config_fingerprint(cfg))
+
+
+def sphere_center(rt: CaseRuntime, t):
+    c = np.asarray(rt.config["ib"]["center"], float)
+    if rt.motion is None:
+        return c
+    return c + rt.motion.centre(t)
+
+
+def diagnostics(rt: CaseRuntime, step, ms_per_step):
+    """A history row (ib_case.py:1129-1224)."""
+    drv, load = rt.driver, rt.loads.latest
+    d = np.zeros(4)
+    import ctypes as C
+    out = (C.c_double * 4)()
+    drv.solver.h.call("pyib_diagnostics", out)
+    d[:] = out[:]
+    fL = drv.ib_force_L
+    lag = (fL * (drv.ib_ds ** 3)[:, None]).sum(axis=0)
+    ff = load["force_fluid"]
+    den = max(float(np.linalg.norm(lag)), float(np.linalg.norm(ff)), 1e-300)
+    balance = float(np.linalg.norm(ff - lag)) / den
+    coef = load["body_force"] / rt.reference_force
+    row = {"step": step, "time": drv.time, "Cd": coef[0], "Cy": coef[1], "Cz": coef[2],
+           "interior_indicator_volume": float(load["indicator_volume"]), "slip_max": d[2], "slip_rms": d[3],
+           "speed_max": d[0], "cfl": d[0] * rt.dt / rt.dx, "mass_residual_inf": d[1],
+           "force_balance_relerr": balance, "ib_force_updates": drv.ib_force_updates_last_step,
+           "helmholtz_iterations": drv.helmholtz_iterations_last_step,
+           "helmholtz_relative_residual": drv.helmholtz_relative_residual_last_step,
+           "helmholtz_tolerance_ratio": drv.helmholtz_tolerance_ratio_last_step,
+           "milliseconds_per_step": ms_per_step}
+    for name, key in (("body_force", "body_force"), ("force_fluid", "force_fluid"),
+                      ("body_moment", "body_moment"), ("moment_fluid", "moment_fluid"),
+                      ("interior_momentum", "linear_momentum")):
+        for a, ax in enumerate("xyz"):
+            row[f"{name}_{ax}"] = float(load[key][a])
+    vals = np.asarray([float(row[c]) for c in HISTORY_COLUMNS])
+    if not np.all(np.isfinite(vals)):
+        raise FloatingPointError(f"non-finite diagnostic at step {step}: {row}")
+    if balance > 1e-9 and rt.config["runtime"]["precision"] == "float64":
+        raise RuntimeError(f"IB force-spread balance failed at step {step}: {balance:.3e}")
+    if row["ib_force_updates"] != 1:
+        raise RuntimeError(f"IB update-count invariant failed at step {step}")
+    return row
+
+
+def _atomic_npz(path: Path, **arrays):
+    tmp = path.with_name(f".{path.stem}.{uuid.uuid4().hex}.tmp.npz")
+    try:
+        np.savez(tmp, **arrays)
+        with tmp.open("r+b") as fh:
+            fh.flush()
+            os.fsync(fh.fileno())
+        os.replace(tmp, path)
+    finally:
+        if tmp.exists():
+            tmp.unlink()
+
+
+def save_checkpoint(path: Path, rt: CaseRuntime, step, s, s_old):
+    drv = rt.driver
+    st = drv.ib_state_dict()
+    cur = rt.loads.current
+    _atomic_npz(path, schema=np.int64(CHECKPOINT_SCHEMA_VERSION), fingerprint=np.bytes_(rt.fingerprint),
+                step=np.int64(step), time=np.float64(drv.time), s=np.asarray(s), s_old=np.asarray(s_old),
+                force_E=st["force_E"], force_L=st["force_L"], force_mode=np.bytes_(st["force_mode"]),
+                force_update_count=np.int64(st["force_update_count"]), loads=np.asarray(cur),
+                device=np.bytes_("b200"), precision=np.bytes_(rt.config["runtime"]["precision"]))
+
+
+def load_checkpoint(path: Path, rt: CaseRuntime):
+    with np.load(path) as d:
+        if int(d["schema"]) != CHECKPOINT_SCHEMA_VERSION:
+            raise CaseConfigError("unsupported checkpoint schema")
+        if bytes(d["fingerprint"]).decode() != rt.fingerprint:
+            raise CaseConfigError("checkpoint was written for a different configuration")
+        lay = rt.layout
+        s, s_old = np.asarray(d["s"]), np.asarray(d["s_old"])
+        if s.shape != (lay.NE,) or s_old.shape != (lay.NE,):
+            raise CaseConfigError("checkpoint layout does not match the configuration")
+        for arr in (s, s_old, d["force_E"], d["force_L"], d["loads"]):
+            if not np.all(np.isfinite(arr)):
+                raise CaseConfigError("checkpoint holds non-finite values")
+        step = int(d["step"])
+        drv = rt.driver
+        drv.time = step * rt.dt
+        drv.load_ib_state_dict({"force_mode": bytes(d["force_mode"]).decode(), "force_E": d["force_E"],
+                                "force_L": d["force_L"], "force_update_count": int(d["force_update_count"])})
+        rt.loads.current = np.asarray(d["loads"])
+        if rt.motion is not None:
+            mk, v = rt.motion(drv.time)
+            drv.set_ib(drv.ib, mk, drv.ib_ds, v)
+    return step, s, s_old
+
+
+def run_case(config, outdir, *, resume=False, overwrite=False, quiet=False):
+    """Run one case; returns a summary dict (ib_case.py:1413-1648)."""
+    rt = build_runtime(config)
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    hist_path, ckpt = out / "history.csv", out / "checkpoint.npz"
+    if not resume and not overwrite and (hist_path.exists() or ckpt.exists()):
+        raise FileExistsError(f"{out} already contains run artifacts; pass overwrite=True or resume=True")
+    drv = rt.driver
+    t_setup = time.perf_counter()
+    if resume:
+        start, s, s_old = load_checkpoint(ckpt, rt)
+        rows = []
+        if hist_path.exists():
+            with hist_path.open() as fh:
+                rows = [r for r in csv.DictReader(fh) if int(float(r["step"])) <= start]
+    else:
+        start = 0
+        s = drv.initial_stream_function(rt.config["physics"]["inflow_speed"])
+        s, _, _ = drv.calc_vel(s)
+        s_old = np.asarray(s).copy()
+        rt.loads.initialize(sphere_center(rt, 0.0))
+        rows = []
+    if start >= rt.steps:
+        raise CaseConfigError(f"target steps ({rt.steps}) must exceed checkpoint step ({start})")
+    meta = {"name": rt.config["name"], "device": "b200", "precision": rt.config["runtime"]["precision"],
+            "fingerprint": rt.fingerprint, "cells": int(rt.layout.cell_active.sum()),
+            "edges": int(rt.layout.edge_exists.sum()), "markers": int(drv.ib_markers.shape[0]),
+            "setup_seconds": time.perf_counter() - t_setup, "start_step": start}
+    (out / "metadata.json").write_text(json.dumps(meta, indent=2) + "\n")
+    fh = hist_path.open("w", newline="")
+    writer = csv.DictWriter(fh, fieldnames=HISTORY_COLUMNS)
+    writer.writeheader()
+    for r in rows:
+        writer.writerow(r)
+    stop = {"flag": False}
+    old = {}
+    for nm in ("SIGTERM", "SIGINT", "SIGUSR1"):
+        if hasattr(signal, nm):
+            sig = getattr(signal, nm)
+            try:
+                old[sig] = signal.getsignal(sig)
+                signal.signal(sig, lambda *_: stop.__setitem__("flag", True))
+            except (OSError, ValueError):
+                pass
+    o = rt.config["output"]
+    done = start
+    t0, s0 = time.perf_counter(), start
+    try:
+        for step in range(start + 1, rt.steps + 1):
+            drv.time = (step - 1) * rt.dt
+            s, vc, s_old = drv.step(s, s_old, rt.dt, rt.dt, inner=rt.inner)
+            drv.time = step * rt.dt
+            rt.loads.advance(sphere_center(rt, drv.time), rt.dt)
+            done = step
+            due = (o["checkpoint_every"] and step % o["checkpoint_every"] == 0) or step == rt.steps \
+                or stop["flag"]
+            if step <= 3 or step % o["sample_every"] == 0 or due:
+                now = time.perf_counter()
+                row = diagnostics(rt, step, (now - t0) * 1000.0 / max(step - s0, 1))
+                t0, s0 = now, step
+                writer.writerow(row)
+                fh.flush()
+                if not quiet:
+                    print(f"step={step:6d} t={row['time']:9.5f} Cd={row['Cd']:10.5f} "
+                          f"CG={row['helmholtz_iterations']:5d} {row['milliseconds_per_step']:8.1f} ms/step",
+                          flush=True)
+            if due:
+                fh.flush()
+                os.fsync(fh.fileno())
+                save_checkpoint(ckpt, rt, step, s, s_old)
+            if stop["flag"]:
+                break
+    finally:
+        fh.close()
+        for sig, h in old.items():
+            try:
+                signal.signal(sig, h)
+            except (OSError, ValueError):
+                pass
+    meta.update(completed_step=done, complete=done == rt.steps)
+    (out / "metadata.json").write_text(json.dumps(meta, indent=2) + "\n")
+    return {"completed_step": done, "stopped": done != rt.steps, "body_force": rt.loads.latest["body_force"]}
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser(description="Run a PyIB case on the B200 path")
+    ap.add_argument("config")
+    ap.add_argument("--outdir", required=True)
+    ap.add_argument("--resume", action="store_true")
+    ap.add_argument("--overwrite", action="store_true")
+    ap.add_argument("--steps", type=int)
+    ap.add_argument("--precision", choices=["float64", "mixed"])
+    a = ap.parse_args(argv)
+    try:
+        cfg = json.loads(Path(a.config).read_text())
+        cfg.setdefault("runtime", {})["device"] = "b200"
+        if a.precision:
+            cfg["runtime"]["precision"] = a.precision
+        if a.steps:
+            cfg.setdefault("time", {})["steps"] = a.steps
+        run_case(cfg, a.outdir, resume=a.resume, overwrite=a.overwrite)
+    except (CaseConfigError, RuntimeError, FloatingPointError, FileExistsError) as exc:
+        print(f"error: {exc}")
+        return 2
+    return 0

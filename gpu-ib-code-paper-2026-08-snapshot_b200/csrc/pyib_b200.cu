@@ -29,7 +29,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 148 * 8;      // fixed grid of the flat vector kernels (148 SMs x 8)
-constexpr int kPartStride = 32768;       // partial-sum slots per reduction value (>= any grid)
+constexpr int kPartStride = 65536;       // partial-sum slots per reduction value (>= any grid)
 constexpr int kSlots = 16;               // reduction values per block
 // structured stencil tiles: 32 x 8 threads in (x, y), each marching KZ planes in z
 constexpr int TX = 32, TY = 8;
@@ -45,6 +45,8 @@ struct LevelMeta {
   long long fbase[3];
   long long ebase[3];
   long long ecount[3];
+  double prec_reg;     // preconditioner value of the level's regular edges
+  int plane_base;      // first per-plane partial-sum slot of this level (kernel RI)
   int zbA;             // first z-block of this level in the cell-tile grids
   int zbR;             // first z-block of this level in the node-tile grid
 };
@@ -53,9 +55,11 @@ struct Meta {
   int nl;
   LevelMeta lv[PYIB_MAX_LEVELS];
   long long nc, nf, ne;
-  int kz;              // z planes marched by one tile
+  int kz;              // z planes marched by one cell tile (kernels A and V)
+  int kzR;             // z planes marched by one node tile (kernel RI)
   int gxA, gyA, gzA;   // cell-tile grid (kernels A and V)
-  int gxR, gyR, gzR;   // node-tile grid (kernel RI), tiles of (TX-1) x (TY-1) nodes
+  int gxR, gyR, gzR;   // node-tile grid (kernel RI)
+  int nplanes;         // per-plane partial sums of kernel RI (independent of the z-chunk depth)
 };
 
 struct CGState {
@@ -63,9 +67,9 @@ struct CGState {
   double true_eta, true_l2, tol1, tol2;
   double rou, kfac;              // V block: rou*v - kfac*(Vd v)
   double thresh_in;              // inner (float32) stop threshold of the mixed solver
-  int m, done, iters, check, cg_max, alpd, pad0, pad1;
+  int m, done, iters, check, cg_max, alpd, stop, pad1;
   unsigned int counter;
-  unsigned int pad2;
+  unsigned int counter2;
 };
 
 struct Table {
@@ -129,6 +133,8 @@ struct pyib_ctx {
   double cg_seconds = 0.0;
   long long cg_iters = 0;
   long long launches = 0;        // kernels launched by this context
+  bool tuned = false;            // matvec tile depths chosen by timing
+  double tune_ms = 0.0;          // best matvec time seen by the tuner
 };
 
 namespace {
@@ -249,6 +255,32 @@ __device__ __forceinline__ int level_of_zblock(const Meta& m, int bz, bool node_
   int L = 0;
   while (L + 1 < m.nl && bz >= (node_grid ? m.lv[L + 1].zbR : m.lv[L + 1].zbA)) ++L;
   return L;
+}
+
+// Grids of the structured kernels for z-chunk depths kzA (cells) and kzR (nodes).
+void set_grids(Meta& m, int kzA, int kzR) {
+  m.kz = kzA;
+  m.kzR = kzR;
+  int zA = 0, zR = 0, gxA = 1, gyA = 1, gxR = 1, gyR = 1;
+  for (int L = 0; L < m.nl; ++L) {
+    LevelMeta& l = m.lv[L];
+    l.zbA = zA;
+    l.zbR = zR;
+    zA += (l.n[2] + kzA - 1) / kzA;
+    zR += (l.n[2] + 1 + kzR - 1) / kzR;
+    gxA = std::max(gxA, (l.n[0] + TX - 1) / TX);
+    gyA = std::max(gyA, (l.n[1] + TY - 1) / TY);
+    gxR = std::max(gxR, (l.n[0] + 1 + TX - 1) / TX);
+    gyR = std::max(gyR, (l.n[1] + 1 + TY - 1) / TY);
+  }
+  m.gxA = gxA; m.gyA = gyA; m.gzA = zA;
+  m.gxR = gxR; m.gyR = gyR; m.gzR = zR;
+  int pb = 0;
+  for (int L = 0; L < m.nl; ++L) {
+    m.lv[L].plane_base = pb;
+    pb += gxR * gyR * (m.lv[L].n[2] + 1);
+  }
+  m.nplanes = pb;
 }
 
 // ---------------------------------------------------------------------------
@@ -387,10 +419,23 @@ __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v
 
 // ---------------------------------------------------------------------------
 // matvec kernel RI: w = R I vq, fused with the dot p.w and alpha = eta / p.w.
-// A 32x8 block covers (TX-1)x(TY-1) node columns plus a one-node halo at -x,-y; each
-// thread forms the three face values F_a = (h/2)(vq_a[lo] + vq_a[hi]) at its node
-// index, shares them through a shared-memory plane, and marches KZ planes in z.
+// Thread (i,j) of a 32x8 node tile marches kz node planes.  The face values
+//   F_x(i,j,k) = (h/2)(vq_x(i-1,j,k) + vq_x(i,j,k)),  F_y likewise in y,
+//   F_z(i,j,k) = (h/2)(vq_z(i,j,k-1) + vq_z(i,j,k))
+// of the node and of its -x and -y neighbours come straight from (L1-cached)
+// loads; the z-lower values are carried from the previous plane.
+//   w_x(i,j,k) = F_z(i,j,k) - F_z(i,j-1,k) + F_y(i,j,k-1) - F_y(i,j,k)
+//   w_y(i,j,k) = F_x(i,j,k) - F_x(i,j,k-1) + F_z(i-1,j,k) - F_z(i,j,k)
+//   w_z(i,j,k) = F_y(i,j,k) - F_y(i-1,j,k) + F_x(i,j-1,k) - F_x(i,j,k)
 // ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T patch_row(const long long* __restrict__ pptr, const int* __restrict__ pcol,
+                                       const T* __restrict__ pval, const T* __restrict__ src, int r) {
+  T acc = 0;
+  for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * src[pcol[q]];
+  return acc;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
                                                    const T* __restrict__ p,
@@ -401,109 +446,109 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
                                                    const T* __restrict__ pval, double* partials,
                                                    CGState* st, int do_dot) {
   if (st->done) return;
-  __shared__ T sF[2][3][TY][TX];
+  __shared__ double sh[32];
+  __shared__ bool last;
   const int L = level_of_zblock(m, blockIdx.z, true);
   const LevelMeta& l = m.lv[L];
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i = blockIdx.x * (TX - 1) + tx - 1, j = blockIdx.y * (TY - 1) + ty - 1;
-  const int k0 = (blockIdx.z - l.zbR) * m.kz;
-  const int k1 = min(k0 + m.kz, nz + 1);
+  const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
+  const int k0 = (blockIdx.z - l.zbR) * m.kzR;
+  const int k1 = min(k0 + m.kzR, nz + 1);
   const long long nc = m.nc;
   const T* vx = vq + l.cbase;
   const T* vy = vq + nc + l.cbase;
   const T* vz = vq + 2 * nc + l.cbase;
   const T hh = (T)(0.5 * l.h);
   const int cs = nx * ny;
-  const bool in_ij = i >= 0 && j >= 0 && i <= nx && j <= ny;
-  const bool own = tx > 0 && ty > 0 && in_ij;
-  const bool cx = i < nx && j < ny;            // cell (i,j,.) exists in x,y
-  const bool cxm = i > 0 && j < ny;            // cell (i-1,j,.)
-  const bool cym = j > 0 && i < nx;            // cell (i,j-1,.)
-  // F at plane k0-1 for the own node (z-direction differences)
-  auto Fx = [&](int k) -> T {   // x-face at node (i,j,k): cells (i-1,j,k),(i,j,k)
-    if (!in_ij || k < 0 || k >= nz || j >= ny) return (T)0;
-    const int o = k * cs + j * nx + i;
-    T a = 0;
-    if (i > 0) a += vx[o - 1];
-    if (i < nx) a += vx[o];
-    return hh * a;
-  };
-  auto Fy = [&](int k) -> T {   // y-face at (i,j,k): cells (i,j-1,k),(i,j,k)
-    if (!in_ij || k < 0 || k >= nz || i >= nx) return (T)0;
-    const int o = k * cs + j * nx + i;
-    T a = 0;
-    if (j > 0) a += vy[o - nx];
-    if (j < ny) a += vy[o];
-    return hh * a;
-  };
-  (void)cx; (void)cxm; (void)cym;
-  T fx_prev = Fx(k0 - 1), fy_prev = Fy(k0 - 1);
-  // vz at (i,j,k0-1) for F_z
-  T vz_prev = (in_ij && i < nx && j < ny && k0 > 0) ? vz[(k0 - 1) * cs + j * nx + i] : (T)0;
-  double dot[1] = {0.0};
-  const int ex_sk = (ny + 1) * nx, ey_sk = ny * (nx + 1), ez_sk = (ny + 1) * (nx + 1);
-  int buf = 0;
+  const bool act = i <= nx && j <= ny;
+  // cell-column validity (x,y) for the cells each face reads
+  const bool c00 = i < nx && j < ny;              // (i, j)
+  const bool cm0 = i > 0 && i <= nx && j < ny;    // (i-1, j)
+  const bool c0m = i < nx && j > 0 && j <= ny;    // (i, j-1)
+  const bool cmm = i > 0 && j > 0 && i <= nx && j <= ny;   // (i-1, j-1)
+  const int o00 = j * nx + i;
+  auto ld = [&](const T* a, bool ok, int o) -> T { return ok ? a[o] : (T)0; };
+  T vz00_m = 0, vzm0_m = 0, vz0m_m = 0;            // z-face inputs at plane k-1
+  T fy_m = 0, fx_m = 0;                            // F_y(i,j,k-1), F_x(i,j,k-1)
+  if (act && k0 > 0) {
+    const int ob = (k0 - 1) * cs + o00;
+    vz00_m = ld(vz, c00, ob);
+    vzm0_m = ld(vz, cm0, ob - 1);
+    vz0m_m = ld(vz, c0m, ob - nx);
+    if (k0 - 1 < nz) {
+      if (i < nx) fy_m = hh * (ld(vy, c0m, ob - nx) + ld(vy, c00, ob));
+      if (j < ny) fx_m = hh * (ld(vx, cm0, ob - 1) + ld(vx, c00, ob));
+    }
+  }
   for (int k = k0; k < k1; ++k) {
-    const T fx = Fx(k), fy = Fy(k);
-    T vz_cur = (in_ij && i < nx && j < ny && k < nz) ? vz[k * cs + j * nx + i] : (T)0;
-    const T fz = hh * (vz_prev + vz_cur);     // z-face at (i,j,k): cells (i,j,k-1),(i,j,k)
-    sF[buf][0][ty][tx] = fx;
-    sF[buf][1][ty][tx] = fy;
-    sF[buf][2][ty][tx] = fz;
-    __syncthreads();
-    if (own) {
-      // w_x(i,j,k) = Fz(i,j,k) - Fz(i,j-1,k) + Fy(i,j,k-1) - Fy(i,j,k)
-      // w_y(i,j,k) = Fx(i,j,k) - Fx(i,j,k-1) + Fz(i-1,j,k) - Fz(i,j,k)
-      // w_z(i,j,k) = Fy(i,j,k) - Fy(i-1,j,k) + Fx(i,j-1,k) - Fx(i,j,k)
-      const T fz_jm = sF[buf][2][ty - 1][tx], fz_im = sF[buf][2][ty][tx - 1];
-      const T fy_im = sF[buf][1][ty][tx - 1], fx_jm = sF[buf][0][ty - 1][tx];
+    double dot[1] = {0.0};
+    if (act) {
+      const bool zin = k < nz;
+      const int ob = k * cs + o00;
+      const T vz00 = zin ? ld(vz, c00, ob) : (T)0;
+      const T vzm0 = zin ? ld(vz, cm0, ob - 1) : (T)0;
+      const T vz0m = zin ? ld(vz, c0m, ob - nx) : (T)0;
+      T fx = 0, fy = 0, fx_jm = 0, fy_im = 0;
+      if (zin) {
+        const T vx00 = ld(vx, c00, ob), vxm0 = ld(vx, cm0, ob - 1);
+        const T vy00 = ld(vy, c00, ob), vy0m = ld(vy, c0m, ob - nx);
+        if (j < ny) fx = hh * (vxm0 + vx00);                                          // F_x(i,j)
+        if (i < nx) fy = hh * (vy0m + vy00);                                          // F_y(i,j)
+        if (j > 0) fx_jm = hh * (ld(vx, cmm, ob - nx - 1) + ld(vx, c0m, ob - nx));    // F_x(i,j-1)
+        if (i > 0) fy_im = hh * (ld(vy, cmm, ob - nx - 1) + ld(vy, cm0, ob - 1));     // F_y(i-1,j)
+      }
+      const T fz = (i < nx && j < ny) ? hh * (vz00_m + vz00) : (T)0;                 // F_z(i,j)
+      const T fz_im = (i > 0 && j < ny) ? hh * (vzm0_m + vzm0) : (T)0;               // F_z(i-1,j)
+      const T fz_jm = (i < nx && j > 0) ? hh * (vz0m_m + vz0m) : (T)0;               // F_z(i,j-1)
       if (i < nx) {
-        long long e = l.ebase[0] + (long long)k * ex_sk + j * nx + i;
-        T val = fz - fz_jm + fy_prev - fy;
-        if (pbits && bit_set(pbits, e)) {
-          const int r = prow[e];
-          T acc = 0;
-          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
-          val = acc;
-        }
+        const long long e = l.ebase[0] + (long long)k * ((ny + 1) * nx) + j * nx + i;
+        T val = fz - fz_jm + fy_m - fy;
+        if (pbits && bit_set(pbits, e)) val = patch_row<T>(pptr, pcol, pval, vq, prow[e]);
         w[e] = val;
         if (do_dot) dot[0] += (double)p[e] * (double)val;
       }
       if (j < ny) {
-        long long e = l.ebase[1] + (long long)k * ey_sk + j * (nx + 1) + i;
-        T val = fx - fx_prev + fz_im - fz;
-        if (pbits && bit_set(pbits, e)) {
-          const int r = prow[e];
-          T acc = 0;
-          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
-          val = acc;
-        }
+        const long long e = l.ebase[1] + (long long)k * (ny * (nx + 1)) + j * (nx + 1) + i;
+        T val = fx - fx_m + fz_im - fz;
+        if (pbits && bit_set(pbits, e)) val = patch_row<T>(pptr, pcol, pval, vq, prow[e]);
         w[e] = val;
         if (do_dot) dot[0] += (double)p[e] * (double)val;
       }
-      if (k < nz) {
-        long long e = l.ebase[2] + (long long)k * ez_sk + j * (nx + 1) + i;
+      if (zin) {
+        const long long e = l.ebase[2] + (long long)k * ((ny + 1) * (nx + 1)) + j * (nx + 1) + i;
         T val = fy - fy_im + fx_jm - fx;
-        if (pbits && bit_set(pbits, e)) {
-          const int r = prow[e];
-          T acc = 0;
-          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vq[pcol[q]];
-          val = acc;
-        }
+        if (pbits && bit_set(pbits, e)) val = patch_row<T>(pptr, pcol, pval, vq, prow[e]);
         w[e] = val;
         if (do_dot) dot[0] += (double)p[e] * (double)val;
       }
+      vz00_m = vz00; vzm0_m = vzm0; vz0m_m = vz0m;
+      fx_m = fx; fy_m = fy;
     }
-    fx_prev = fx;
-    fy_prev = fy;
-    vz_prev = vz_cur;
-    buf ^= 1;
+    if (do_dot) {
+      // one partial per (level, tile, plane): the sum does not depend on the z-chunk depth
+      block_sum<1>(dot, sh);
+      if (threadIdx.x == 0 && threadIdx.y == 0)
+        partials[l.plane_base + (k * m.gyR + blockIdx.y) * m.gxR + blockIdx.x] = dot[0];
+    }
   }
   if (!do_dot) return;
-  if (grid_sum<1>(dot, partials, &st->counter)) {
-    st->pw = dot[0];
-    st->alpha = st->eta / (dot[0] != 0.0 ? dot[0] : INFINITY);
+  const int tid = threadIdx.x + TX * threadIdx.y;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+    last = atomicAdd(&st->counter, 1u) == nb - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // every slot in [0, nplanes) was written by exactly one block of this launch
+  double acc[1] = {0.0};
+  for (int q = tid; q < m.nplanes; q += TX * TY) acc[0] += ((volatile double*)partials)[q];
+  block_sum<1>(acc, sh);
+  if (tid == 0) {
+    st->pw = acc[0];
+    st->alpha = st->eta / (acc[0] != 0.0 ? acc[0] : INFINITY);
+    st->counter = 0u;
   }
 }
 
@@ -537,12 +582,24 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(long long ne, const double
     st->m = 0;
     st->done = 0;
     st->iters = 0;
+    st->stop = 0;
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_cg_update(long long ne, double* x, double* r,
-                                                        const double* __restrict__ p,
+// Preconditioner value of edge e: the level's regular value unless the edge is flagged.
+__device__ __forceinline__ double prec_of(const Meta& m, const unsigned int* __restrict__ bits,
+                                          const double* __restrict__ prec, long long e) {
+  if (bit_set(bits, e)) return prec[e];
+  int L = 0;
+  while (L + 1 < m.nl && e >= m.lv[L + 1].ebase[0]) ++L;
+  return m.lv[L].prec_reg;
+}
+
+// r -= alpha w on unmasked edges; eta' = sum (r*prec)*r; the last block applies the
+// stopping test (every `check` iterations, or at cg_max) and sets `stop`.
+__global__ void __launch_bounds__(kThreads) k_cg_update(Meta m, long long ne, double* r,
                                                         const double* __restrict__ w,
+                                                        const unsigned int* __restrict__ pbits,
                                                         const double* __restrict__ prec,
                                                         double* partials, CGState* st) {
   if (st->done) return;
@@ -550,27 +607,26 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(long long ne, double* x,
   double v[1] = {0.0};
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
-    const double pr = prec[e];
-    x[e] += alpha * p[e];
+    const double pr = prec_of(m, pbits, prec, e);
     if (pr != 0.0) {
       const double re = r[e] - alpha * w[e];
       r[e] = re;
       v[0] += (re * pr) * re;
     }
   }
-  if (grid_sum<1>(v, partials, &st->counter) && threadIdx.x == 0) {
+  if (grid_sum<1>(v, partials, &st->counter)) {
     const double en = v[0];
     st->eta_new = en;
-    const int m = st->m + 1;
-    st->m = m;
+    const int mm = st->m + 1;
+    st->m = mm;
     bool stop = false;
-    if (m % st->check == 0) {
+    if (mm % st->check == 0) {
       if (!isfinite(en) || en < st->thresh) stop = true;
     }
-    if (m >= st->cg_max) stop = true;
+    if (mm >= st->cg_max) stop = true;
     if (stop) {
-      st->done = 1;
-      st->iters = m;
+      st->stop = 1;
+      st->iters = mm;
     } else {
       st->beta = en / (st->eta != 0.0 ? st->eta : INFINITY);
       st->eta = en;
@@ -578,14 +634,33 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(long long ne, double* x,
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_cg_p(long long ne, const double* __restrict__ r,
-                                                   const double* __restrict__ prec, double* p,
-                                                   const CGState* st) {
+// x += alpha p (the iterate of this iteration), then p = r*prec + beta p unless the
+// stopping test fired; the last block turns `stop` into `done`.
+__global__ void __launch_bounds__(kThreads) k_cg_p(Meta m, long long ne, const double* __restrict__ r,
+                                                   const unsigned int* __restrict__ pbits,
+                                                   const double* __restrict__ prec, double* p, double* x,
+                                                   CGState* st) {
   if (st->done) return;
-  const double beta = st->beta;
+  const double alpha = st->alpha, beta = st->beta;
+  const bool stop = st->stop != 0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x)
-    p[e] = r[e] * prec[e] + beta * p[e];
+       e += (long long)gridDim.x * blockDim.x) {
+    const double pe = p[e];
+    x[e] += alpha * pe;
+    if (!stop) p[e] = r[e] * prec_of(m, pbits, prec, e) + beta * pe;
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int t = atomicAdd(&st->counter2, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    st->counter2 = 0u;
+    if (stop) st->done = 1;
+  }
 }
 
 __global__ void k_mask(long long n, const double* __restrict__ prec, double* w) {
@@ -1128,7 +1203,7 @@ size_t table_elem(int t) {
     case PYIB_T_PREC: case PYIB_T_INLET_VAL: case PYIB_T_CURL_VAL: case PYIB_T_ROT_VAL:
     case PYIB_T_P_VAL3: case PYIB_T_I_VAL3: case PYIB_T_F_AOL: case PYIB_T_VOLCI:
     case PYIB_T_BF_AF: case PYIB_T_PA_VAL: case PYIB_T_PV_VAL: case PYIB_T_PR_VAL:
-    case PYIB_T_LC_CPOS:
+    case PYIB_T_LC_CPOS: case PYIB_T_PREC_REG:
       return 8;
     case PYIB_T_CURL_PTR: case PYIB_T_ROT_PTR: case PYIB_T_P_PTR: case PYIB_T_I_PTR:
     case PYIB_T_CF_PTR: case PYIB_T_PA_PTR: case PYIB_T_PV_PTR: case PYIB_T_PR_PTR:
@@ -1160,7 +1235,7 @@ int check_dev_err(pyib_ctx* ctx) {
 }
 
 bool tables_ready(pyib_ctx* c) {
-  const int need[] = {PYIB_T_PREC, PYIB_T_CURL_PTR, PYIB_T_ROT_PTR, PYIB_T_P_PTR, PYIB_T_I_PTR,
+  const int need[] = {PYIB_T_PREC, PYIB_T_PREC_BITS, PYIB_T_PREC_REG, PYIB_T_CURL_PTR, PYIB_T_ROT_PTR, PYIB_T_P_PTR, PYIB_T_I_PTR,
                       PYIB_T_CF_PTR, PYIB_T_F_LO, PYIB_T_F_HI, PYIB_T_F_AOL, PYIB_T_VOLCI};
   for (int t : need)
     if (!c->tab[t].ptr) return false;
@@ -1263,6 +1338,54 @@ int launch_matvec(pyib_ctx* ctx, const double* in, double* out, int alpd, int do
                                  tp<double>(ctx, PYIB_T_PR_VAL));
 }
 
+// Autotuner: time the float64 matvec for every pair of z-chunk depths (cells, nodes)
+// and keep the fastest.  Runs once per context, before any CG graph is captured.
+int tune_matvec(pyib_ctx* ctx) {
+  if (ctx->tuned) return PYIB_OK;
+  CGState h{};
+  CK(cudaMemcpyAsync(&h, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CGState t = h;
+  t.rou = 1.0;
+  t.kfac = 1e-3;
+  t.done = 0;
+  t.counter = 0u;
+  CK(cudaMemcpyAsync(ctx->st, &t, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  const int depths[5] = {1, 2, 4, 8, 16};
+  const Meta base = ctx->meta;
+  int bestA = base.kz, bestR = base.kzR;
+  double best = 1e30;
+  for (int a = 0; a < 5; ++a) {
+    for (int b = 0; b < 5; ++b) {
+      Meta m2 = base;
+      set_grids(m2, depths[a], depths[b]);
+      if ((long long)m2.gxR * m2.gyR * m2.gzR > kPartStride) continue;
+      ctx->meta = m2;
+      RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
+      CK(cudaEventRecord(ctx->ev0, ctx->stream));
+      for (int q = 0; q < 3; ++q) RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
+      CK(cudaEventRecord(ctx->ev1, ctx->stream));
+      CK(cudaEventSynchronize(ctx->ev1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (ms < best) {
+        best = ms;
+        bestA = depths[a];
+        bestR = depths[b];
+      }
+    }
+  }
+  ctx->meta = base;
+  set_grids(ctx->meta, bestA, bestR);
+  ctx->tune_ms = best / 3.0;
+  ctx->tuned = true;
+  ctx->cg_graph_check = -1;
+  ctx->mix_graph_check = -1;
+  CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PYIB_OK;
+}
+
 int set_state_solver(pyib_ctx* ctx, double dt, int alpd) {
   CGState h{};
   CK(cudaMemcpyAsync(&h, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1275,7 +1398,9 @@ int set_state_solver(pyib_ctx* ctx, double dt, int alpd) {
   h.cg_max = ctx->prm.cg_max;
   h.alpd = alpd;
   h.done = 0;
+  h.stop = 0;
   h.counter = 0u;
+  h.counter2 = 0u;
   CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
   return PYIB_OK;
 }
@@ -1290,12 +1415,13 @@ int masked_matvec(pyib_ctx* ctx, const double* in, double* out, double dt, int a
 int cg_iteration(pyib_ctx* ctx) {
   RET(launch_matvec(ctx, ctx->p, ctx->w, 1, 1));
   const long long ne = ctx->lay.nedge;
-  k_cg_update<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x, ctx->r, ctx->p, ctx->w,
+  const unsigned int* pb = tp<unsigned int>(ctx, PYIB_T_PREC_BITS);
+  k_cg_update<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ctx->meta, ne, ctx->r, ctx->w, pb,
                                                           tp<double>(ctx, PYIB_T_PREC), ctx->partials,
                                                           ctx->st);
   CKL();
-  k_cg_p<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, tp<double>(ctx, PYIB_T_PREC), ctx->p,
-                                                     ctx->st);
+  k_cg_p<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ctx->meta, ne, ctx->r, pb, tp<double>(ctx, PYIB_T_PREC),
+                                                     ctx->p, ctx->x, ctx->st);
   CKL();
   return PYIB_OK;
 }
@@ -1324,6 +1450,7 @@ int build_cg_graph(pyib_ctx* ctx) {
 int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
+  RET(tune_matvec(ctx));
   RET(set_state_solver(ctx, dt, 1));
   RET(build_cg_graph(ctx));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -1507,6 +1634,7 @@ int clear_done(pyib_ctx* ctx) {
 int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
+  RET(tune_matvec(ctx));
   RET(ensure_mixed(ctx));
   RET(build_diag(ctx));
   const double kfac = 0.5 * dt * ctx->prm.visc;
@@ -1765,7 +1893,8 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
   }
   m.nc = cb; m.nf = fb; m.ne = eb;
   {
-    // z-chunk depth: the deepest of 16, 8, 4, 2, 1 planes that still yields enough tiles
+    // default z-chunk depth: the deepest of 16, 8, 4, 2, 1 planes that still yields
+    // enough tiles (the autotuner may change it, see tune_matvec)
     long long plane_tiles = 0;
     for (int L = 0; L < m.nl; ++L) {
       const LevelMeta& l = m.lv[L];
@@ -1773,22 +1902,8 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
     }
     int kz = 16;
     while (kz > 1 && plane_tiles / kz < kTargetBlocks) kz >>= 1;
-    m.kz = kz;
-    int zA = 0, zR = 0, gxA = 1, gyA = 1, gxR = 1, gyR = 1;
-    for (int L = 0; L < m.nl; ++L) {
-      LevelMeta& l = m.lv[L];
-      l.zbA = zA;
-      l.zbR = zR;
-      zA += (l.n[2] + kz - 1) / kz;
-      zR += (l.n[2] + 1 + kz - 1) / kz;
-      gxA = std::max(gxA, (l.n[0] + TX - 1) / TX);
-      gyA = std::max(gyA, (l.n[1] + TY - 1) / TY);
-      gxR = std::max(gxR, (l.n[0] + TX - 1) / (TX - 1));
-      gyR = std::max(gyR, (l.n[1] + TY - 1) / (TY - 1));
-    }
-    m.gxA = gxA; m.gyA = gyA; m.gzA = zA;
-    m.gxR = gxR; m.gyR = gyR; m.gzR = zR;
-    if ((long long)gxR * gyR * zR > kPartStride || (long long)gxA * gyA * zA > (1LL << 31)) {
+    set_grids(m, kz, kz);
+    if ((long long)m.gxR * m.gyR * m.gzR > kPartStride) {
       delete ctx;
       return PYIB_E_ARG;
     }
@@ -1884,6 +1999,10 @@ int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes) {
       if (n > 0) { k_d2f<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, (const double*)t.ptr, *f); CKL(); }
     }
   }
+  if (table == PYIB_T_PREC_REG) {
+    if (bytes != (size_t)ctx->meta.nl * 8) return set_err(ctx, PYIB_E_ARG, "PREC_REG needs one value per level");
+    for (int L = 0; L < ctx->meta.nl; ++L) ctx->meta.lv[L].prec_reg = ((const double*)host)[L];
+  }
   if (table == PYIB_T_INLET_IDX) ctx->n_inlet = bytes / 4;
   if (table == PYIB_T_BF_FACE) ctx->n_bf = bytes / 4;
   if (table == PYIB_T_LC_CAND) ctx->n_cand = bytes / 4;
@@ -1892,6 +2011,7 @@ int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes) {
   ctx->mix_graph_check = -1;
   ctx->diag_ready = false;
   ctx->diag_for_kfac = -1.0;
+  ctx->tuned = false;
   return PYIB_OK;
 }
 
@@ -2131,6 +2251,8 @@ int pyib_cg_timing(pyib_ctx* ctx, double* out, int32_t reset) {
   out[0] = ctx->cg_seconds;
   out[1] = (double)ctx->cg_iters;
   out[2] = (double)ctx->launches;
+  out[3] = (double)ctx->meta.kz;
+  out[4] = (double)ctx->meta.kzR;
   if (reset) {
     ctx->cg_seconds = 0.0;
     ctx->cg_iters = 0;
@@ -2162,6 +2284,7 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
   if (!ctx || reps <= 0 || !ms_per) return PYIB_E_ARG;
   if (!tables_ready(ctx) || !ctx->have_params) return set_err(ctx, PYIB_E_STATE, "context not ready");
   CK(cudaSetDevice(ctx->device));
+  RET(tune_matvec(ctx));
   RET(set_state_solver(ctx, dt, 1));
   RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));   // warm
   CK(cudaEventRecord(ctx->ev0, ctx->stream));

@@ -103,6 +103,19 @@ class DeviceSolver:
         lay, ops, h = self.lay, self.ops, self.h
         NC, NF, NE = lay.NC, lay.NF, lay.NE
         h.upload("PREC", self.prec)
+        # per level, the value of the regular edges; edges that differ are flagged
+        reg = np.zeros(lay.N)
+        irregular = np.zeros(NE, dtype=bool)
+        for lv in lay.levels:
+            lo_e = lay.edge_base[lv.L][0]
+            hi_e = lay.edge_base[lv.L][2] + int(np.prod(lv.edge_dims(2)))
+            vals, counts = np.unique(self.prec[lo_e:hi_e], return_counts=True)
+            nz = vals != 0.0
+            reg[lv.L] = vals[nz][np.argmax(counts[nz])] if nz.any() else 0.0
+            irregular[lo_e:hi_e] = self.prec[lo_e:hi_e] != reg[lv.L]
+        h.upload("PREC_BITS", _bits(irregular))
+        h.upload("PREC_REG", reg)
+        self.prec_regular = reg
         ie = np.nonzero(self.inlet)[0]
         hz = np.where(lay.edge_axis[ie] == 2, lay.edge_h[ie], 0.0)
         h.upload("INLET_IDX", ie.astype(np.int32))

@@ -114,6 +114,8 @@ enum pyib_table {
   PYIB_T_PR_BITS, PYIB_T_PR_ROW, PYIB_T_PR_PTR, PYIB_T_PR_COL, PYIB_T_PR_VAL, /* matvec patch RI */
   PYIB_T_LC_CAND, PYIB_T_LC_FIDX,                        /* load-correction cell lists  */
   PYIB_T_LC_CPOS,                                        /* f64[ncell*3] cell centres   */
+  PYIB_T_PREC_BITS,         /* u32 bitmask: edges whose PREC differs from their level's value */
+  PYIB_T_PREC_REG,          /* f64[nlevels] PREC of a level's regular edges              */
   PYIB_T_COUNT
 };
 
@@ -209,7 +211,8 @@ int pyib_diagnostics(pyib_ctx* ctx, double* out);
 
 /* Device timing of the CG solves since the last reset: out[0] CG seconds
  * (CUDA events around each solve), out[1] CG iterations, out[2] kernels launched
- * by this context. */
+ * by this context, out[3] and out[4] the z-chunk depths of the cell and node
+ * stencil tiles the autotuner picked (out holds 5 doubles). */
 int pyib_cg_timing(pyib_ctx* ctx, double* out, int32_t reset);
 /* CUDA events on the context's stream: which=0 records the start, which=1 records
  * the end, waits for it and returns the elapsed milliseconds. */
