@@ -315,9 +315,12 @@ def run_b200(args, world, rank, local):
     t_e2e = time.perf_counter() - t0
     clocks = sampler.stop()
     # standalone matvec timing
-    mv_ms = C.c_double(0.0)
+    mv = (C.c_double * 7)()
     sv.set("WORK_E", np.random.default_rng(0).standard_normal(sv.lay.NE) * sv.lay.edge_exists)
-    sv.h.call("pyib_bench_matvec", 50, C.c_double(run.dt), C.byref(mv_ms))
+    sv.h.call("pyib_bench_matvec", 50, C.c_double(run.dt), mv)
+    mv_ms = C.c_double(mv[0])
+    mv_kernels = dict(zip(["curl_interp", "curl_interp_patch", "viscous", "viscous_patch", "integr_rot_dot",
+                           "integr_rot_patch_reduce"], [float(x) for x in mv[1:7]]))
     ne = int(sv.lay.edge_exists.sum())
     t_dev_max = reduce_max(dist, t_dev)
     t_e2e_max = reduce_max(dist, t_e2e)
@@ -356,7 +359,7 @@ def run_b200(args, world, rank, local):
                          "algorithmic_bytes_per_launch": ALGO_BYTES_PER_EDGE_ITER * ne,
                          "peak_kind": peak_kind},
             "matvec": {"ms": mv_ms.value, "achieved_gbs": mv_achieved, "frac": mv_achieved / peak,
-                       "algorithmic_bytes": ALGO_BYTES_PER_EDGE_MATVEC * ne},
+                       "algorithmic_bytes": ALGO_BYTES_PER_EDGE_MATVEC * ne, "kernel_ms": mv_kernels},
             "cg": {"seconds": cg_s, "iterations": cg_it, "ms_per_iteration": 1e3 * t_iter,
                    "gbs": achieved},
             "gpu_launches": launches,

@@ -26,7 +26,7 @@ TABLES = [
     "PA_BITS", "PA_ROW", "PA_PTR", "PA_COL", "PA_VAL",
     "PV_BITS", "PV_ROW", "PV_PTR", "PV_COL", "PV_VAL",
     "PR_BITS", "PR_ROW", "PR_PTR", "PR_COL", "PR_VAL",
-    "LC_CAND", "LC_FIDX", "LC_CPOS", "PREC_BITS", "PREC_REG",
+    "LC_CAND", "LC_FIDX", "LC_CPOS", "PREC_BITS", "PREC_REG", "PA_IDS", "PV_IDS", "PR_IDS",
 ]
 T = {name: i for i, name in enumerate(TABLES)}
 

@@ -179,6 +179,12 @@ int grid_for(long long n) {
   return (int)b;
 }
 
+// one thread per patch row, every row at once: fixed for a given row count
+int patch_grid(long long rows) {
+  long long b = (rows + kThreads - 1) / kThreads;
+  return (int)(b < 1 ? 1 : b);
+}
+
 // ---------------------------------------------------------------------------
 // deterministic block reduction
 // ---------------------------------------------------------------------------
@@ -205,6 +211,24 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh /*[NV*32]*
   __syncthreads();
 }
 
+// Sum of partials[base + b] for b in [0, n) by one block: each thread adds its
+// stride-blockDim subsequence into four accumulators (L2 loads, independent, so they
+// pipeline), then the block tree.  Fixed order for a given n and block size.
+__device__ __forceinline__ double strided_sum(const double* partials, int n) {
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int q = tid;
+  for (; q + 3 * nt < n; q += 4 * nt) {
+    a0 += __ldcg(partials + q);
+    a1 += __ldcg(partials + q + nt);
+    a2 += __ldcg(partials + q + 2 * nt);
+    a3 += __ldcg(partials + q + 3 * nt);
+  }
+  for (; q < n; q += nt) a0 += __ldcg(partials + q);
+  return (a0 + a1) + (a2 + a3);
+}
+
 // Writes this block's partials; returns true in the block that finishes last,
 // whose thread 0 then holds the totals in v (summed in block order).
 template <int NV>
@@ -228,11 +252,8 @@ __device__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counte
   __threadfence();
   double acc[NV];
 #pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    double t = 0.0;
-    for (unsigned int b = tid; b < nb; b += nthr) t += ((volatile double*)partials)[q * kPartStride + b];
-    acc[q] = t;
-  }
+  for (int q = 0; q < NV; ++q) acc[q] = strided_sum(partials + (size_t)q * kPartStride, (int)nb);
+  (void)nthr;
   block_sum<NV>(acc, sh);
   if (tid == 0) {
 #pragma unroll
@@ -323,26 +344,17 @@ __global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p
     const T ex01 = ex[ox + sxk], ex11 = ex[ox + sxk + nx];
     const T ey01 = ey[oy + syk], ey11 = ey[oy + syk + 1];
     if (!(col_hole && k >= l.hole_lo[2] && k < l.hole_hi[2])) {
-      if (pbits && bit_set(pbits, c)) {
-        const int r = prow[c];
-        for (int d = 0; d < 3; ++d) {
-          T acc = 0;
-          const long long rr = r + d * nA;
-          for (long long q = pptr[rr]; q < pptr[rr + 1]; ++q) acc += pval[q] * p[pcol[q]];
-          vc[d * nc + c] = acc;
-        }
-      } else {
-        const T ez00 = ez[oz], ez10 = ez[oz + 1], ez01 = ez[oz + nx + 1], ez11 = ez[oz + nx + 2];
-        const T ux0 = ey00 + ez01 - ey01 - ez00;
-        const T ux1 = ey10 + ez11 - ey11 - ez10;
-        const T uy0 = ez00 + ex01 - ez10 - ex00;
-        const T uy1 = ez01 + ex11 - ez11 - ex10;
-        const T uz0 = ex00 + ey10 - ex10 - ey00;
-        const T uz1 = ex01 + ey11 - ex11 - ey01;
-        vc[c] = (ux0 + ux1) * s;
-        vc[nc + c] = (uy0 + uy1) * s;
-        vc[2 * nc + c] = (uz0 + uz1) * s;
-      }
+      // template for every cell; rows of irregular cells are overwritten by k_patchA
+      const T ez00 = ez[oz], ez10 = ez[oz + 1], ez01 = ez[oz + nx + 1], ez11 = ez[oz + nx + 2];
+      const T ux0 = ey00 + ez01 - ey01 - ez00;
+      const T ux1 = ey10 + ez11 - ey11 - ez10;
+      const T uy0 = ez00 + ex01 - ez10 - ex00;
+      const T uy1 = ez01 + ex11 - ez11 - ex10;
+      const T uz0 = ex00 + ey10 - ex10 - ey00;
+      const T uz1 = ex01 + ey11 - ex11 - ey01;
+      vc[c] = (ux0 + ux1) * s;
+      vc[nc + c] = (uy0 + uy1) * s;
+      vc[2 * nc + c] = (uz0 + uz1) * s;
     }
     ex00 = ex01; ex10 = ex11; ey00 = ey01; ey10 = ey11;
   }
@@ -388,28 +400,19 @@ __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v
 #pragma unroll
     for (int d = 0; d < 3; ++d) vp[d] = k + 1 < nz ? v[d * nc + c + cstep] : (T)0;
     if (!(col_hole && k >= l.hole_lo[2] && k < l.hole_hi[2])) {
-      if (pbits && bit_set(pbits, c)) {
-        const int r = prow[c];
-        for (int d = 0; d < 3; ++d) {
-          T acc = 0;
-          const T* vd = v + d * nc;
-          for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * vd[pcol[q]];
-          vq[d * nc + c] = rou * v0[d] - kf * acc;
-        }
-      } else {
+      // template for every cell; rows of irregular cells are overwritten by k_patchV
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const T* vd = v + d * nc;
-          const T vc0 = v0[d];
-          T acc = 0;
-          acc += xp ? vd[c + 1] - vc0 : -2 * vc0;
-          acc += xm ? vd[c - 1] - vc0 : -2 * vc0;
-          acc += yp ? vd[c + nx] - vc0 : -2 * vc0;
-          acc += ym ? vd[c - nx] - vc0 : -2 * vc0;
-          acc += (k + 1 < nz) ? vp[d] - vc0 : -2 * vc0;
-          acc += (k > 0) ? vm[d] - vc0 : -2 * vc0;
-          vq[d * nc + c] = rou * vc0 - kf * (acc * inv_h2);
-        }
+      for (int d = 0; d < 3; ++d) {
+        const T* vd = v + d * nc;
+        const T vc0 = v0[d];
+        T acc = 0;
+        acc += xp ? vd[c + 1] - vc0 : -2 * vc0;
+        acc += xm ? vd[c - 1] - vc0 : -2 * vc0;
+        acc += yp ? vd[c + nx] - vc0 : -2 * vc0;
+        acc += ym ? vd[c - nx] - vc0 : -2 * vc0;
+        acc += (k + 1 < nz) ? vp[d] - vc0 : -2 * vc0;
+        acc += (k > 0) ? vm[d] - vc0 : -2 * vc0;
+        vq[d * nc + c] = rou * vc0 - kf * (acc * inv_h2);
       }
     }
 #pragma unroll
@@ -428,13 +431,6 @@ __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v
 //   w_y(i,j,k) = F_x(i,j,k) - F_x(i,j,k-1) + F_z(i-1,j,k) - F_z(i,j,k)
 //   w_z(i,j,k) = F_y(i,j,k) - F_y(i-1,j,k) + F_x(i,j-1,k) - F_x(i,j,k)
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T patch_row(const long long* __restrict__ pptr, const int* __restrict__ pcol,
-                                       const T* __restrict__ pval, const T* __restrict__ src, int r) {
-  T acc = 0;
-  for (long long q = pptr[r]; q < pptr[r + 1]; ++q) acc += pval[q] * src[pcol[q]];
-  return acc;
-}
 
 template <typename T>
 __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
@@ -446,8 +442,8 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
                                                    const T* __restrict__ pval, double* partials,
                                                    CGState* st, int do_dot) {
   if (st->done) return;
-  __shared__ double sh[32];
-  __shared__ bool last;
+  static_assert(TY == 8, "the per-plane combine below assumes 8 warps per block");
+  __shared__ double swarp[16][TY];
   const int L = level_of_zblock(m, blockIdx.z, true);
   const LevelMeta& l = m.lv[L];
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
@@ -485,6 +481,16 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
     if (act) {
       const bool zin = k < nz;
       const int ob = k * cs + o00;
+      const long long ex_e = l.ebase[0] + (long long)k * ((ny + 1) * nx) + j * nx + i;
+      const long long ey_e = l.ebase[1] + (long long)k * (ny * (nx + 1)) + j * (nx + 1) + i;
+      const long long ez_e = l.ebase[2] + (long long)k * ((ny + 1) * (nx + 1)) + j * (nx + 1) + i;
+      // loads that do not depend on the stencil: bitmask words and the dot's p values
+      const unsigned int bwx = (pbits && i < nx) ? pbits[ex_e >> 5] : 0u;
+      const unsigned int bwy = (pbits && j < ny) ? pbits[ey_e >> 5] : 0u;
+      const unsigned int bwz = (pbits && zin) ? pbits[ez_e >> 5] : 0u;
+      const T px = (do_dot && i < nx) ? p[ex_e] : (T)0;
+      const T py = (do_dot && j < ny) ? p[ey_e] : (T)0;
+      const T pz = (do_dot && zin) ? p[ez_e] : (T)0;
       const T vz00 = zin ? ld(vz, c00, ob) : (T)0;
       const T vzm0 = zin ? ld(vz, cm0, ob - 1) : (T)0;
       const T vz0m = zin ? ld(vz, c0m, ob - nx) : (T)0;
@@ -500,52 +506,123 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
       const T fz = (i < nx && j < ny) ? hh * (vz00_m + vz00) : (T)0;                 // F_z(i,j)
       const T fz_im = (i > 0 && j < ny) ? hh * (vzm0_m + vzm0) : (T)0;               // F_z(i-1,j)
       const T fz_jm = (i < nx && j > 0) ? hh * (vz0m_m + vz0m) : (T)0;               // F_z(i,j-1)
+      // template for every edge; irregular edges are overwritten by k_patchRI, which
+      // also adds their share of the dot product
       if (i < nx) {
-        const long long e = l.ebase[0] + (long long)k * ((ny + 1) * nx) + j * nx + i;
-        T val = fz - fz_jm + fy_m - fy;
-        if (pbits && bit_set(pbits, e)) val = patch_row<T>(pptr, pcol, pval, vq, prow[e]);
-        w[e] = val;
-        if (do_dot) dot[0] += (double)p[e] * (double)val;
+        const T val = fz - fz_jm + fy_m - fy;
+        w[ex_e] = val;
+        if (!((bwx >> (ex_e & 31)) & 1u)) dot[0] += (double)px * (double)val;
       }
       if (j < ny) {
-        const long long e = l.ebase[1] + (long long)k * (ny * (nx + 1)) + j * (nx + 1) + i;
-        T val = fx - fx_m + fz_im - fz;
-        if (pbits && bit_set(pbits, e)) val = patch_row<T>(pptr, pcol, pval, vq, prow[e]);
-        w[e] = val;
-        if (do_dot) dot[0] += (double)p[e] * (double)val;
+        const T val = fx - fx_m + fz_im - fz;
+        w[ey_e] = val;
+        if (!((bwy >> (ey_e & 31)) & 1u)) dot[0] += (double)py * (double)val;
       }
       if (zin) {
-        const long long e = l.ebase[2] + (long long)k * ((ny + 1) * (nx + 1)) + j * (nx + 1) + i;
-        T val = fy - fy_im + fx_jm - fx;
-        if (pbits && bit_set(pbits, e)) val = patch_row<T>(pptr, pcol, pval, vq, prow[e]);
-        w[e] = val;
-        if (do_dot) dot[0] += (double)p[e] * (double)val;
+        const T val = fy - fy_im + fx_jm - fx;
+        w[ez_e] = val;
+        if (!((bwz >> (ez_e & 31)) & 1u)) dot[0] += (double)pz * (double)val;
       }
       vz00_m = vz00; vzm0_m = vzm0; vz0m_m = vz0m;
       fx_m = fx; fy_m = fy;
     }
     if (do_dot) {
-      // one partial per (level, tile, plane): the sum does not depend on the z-chunk depth
-      block_sum<1>(dot, sh);
-      if (threadIdx.x == 0 && threadIdx.y == 0)
-        partials[l.plane_base + (k * m.gyR + blockIdx.y) * m.gxR + blockIdx.x] = dot[0];
+      // warp sum of this plane, kept per (plane, warp) until the end of the block
+      double t = dot[0];
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (threadIdx.x == 0) swarp[k - k0][threadIdx.y] = t;
     }
   }
   if (!do_dot) return;
+  __syncthreads();
+  // one partial per (level, tile, plane), combined in a fixed order: the sum does not
+  // depend on the z-chunk depth the autotuner picked
   const int tid = threadIdx.x + TX * threadIdx.y;
-  if (tid == 0) {
+  if (tid < k1 - k0) {
+    const double* q = swarp[tid];
+    const double v = ((q[0] + q[4]) + (q[2] + q[6])) + ((q[1] + q[5]) + (q[3] + q[7]));
+    partials[l.plane_base + ((k0 + tid) * m.gyR + blockIdx.y) * m.gxR + blockIdx.x] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Patch kernels: exact CSR rows of the entities the templates cannot reproduce
+// (interfaces between levels, hole surfaces, collapsed edges).  One thread per
+// row and a grid that covers every row at once: rows are short (about 8
+// entries), so the cost is one dependent gather chain per row, overlapped
+// across all rows.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T csr_row(const long long* __restrict__ ptr, const int* __restrict__ col,
+                                     const T* __restrict__ val, const T* __restrict__ src, long long r) {
+  const long long q0 = ptr[r], q1 = ptr[r + 1];
+  T acc = 0;
+  for (long long q = q0; q < q1; ++q) acc += val[q] * src[col[q]];
+  return acc;
+}
+
+// vc rows: row q = d*nA + r holds component d of cell ids[r]
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_patchA(long long nA, const int* __restrict__ ids,
+                                                     const long long* __restrict__ ptr,
+                                                     const int* __restrict__ col, const T* __restrict__ val,
+                                                     const T* __restrict__ p, T* vc, long long nc,
+                                                     const CGState* __restrict__ st) {
+  if (st->done) return;
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= 3 * nA) return;
+  vc[(q / nA) * nc + ids[q % nA]] = csr_row<T>(ptr, col, val, p, q);
+}
+
+// vq rows: the same Vd row for the three components of cell ids[r]
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __restrict__ ids,
+                                                     const long long* __restrict__ ptr,
+                                                     const int* __restrict__ col, const T* __restrict__ val,
+                                                     const T* __restrict__ v, T* vq, long long nc,
+                                                     const CGState* __restrict__ st) {
+  if (st->done) return;
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= 3 * nV) return;
+  const long long d = q / nV, r = q % nV;
+  const int c = ids[r];
+  const T* vd = v + d * nc;
+  vq[d * nc + c] = (T)st->rou * vd[c] - (T)st->kfac * csr_row<T>(ptr, col, val, vd, r);
+}
+
+// w rows (columns index the component-major vq), plus their share of p.w; the last
+// block sums the per-plane partials of k_mvRI and this kernel's per-block partials
+// in a fixed order and sets alpha = eta / p.w.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* __restrict__ ids,
+                                                      const long long* __restrict__ ptr,
+                                                      const int* __restrict__ col, const T* __restrict__ val,
+                                                      const T* __restrict__ vq, T* w, const T* __restrict__ p,
+                                                      double* partials, int nplanes, CGState* st, int do_dot) {
+  if (st->done) return;
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double dot[1] = {0.0};
+  if (r < nR) {
+    const int e = ids[r];
+    const T acc = csr_row<T>(ptr, col, val, vq, r);
+    w[e] = acc;
+    if (do_dot) dot[0] = (double)p[e] * (double)acc;
+  }
+  if (!do_dot) return;
+  __shared__ double sh[32];
+  __shared__ bool last;
+  block_sum<1>(dot, sh);
+  if (threadIdx.x == 0) {
+    partials[nplanes + blockIdx.x] = dot[0];
     __threadfence();
-    const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
-    last = atomicAdd(&st->counter, 1u) == nb - 1;
+    last = atomicAdd(&st->counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // every slot in [0, nplanes) was written by exactly one block of this launch
-  double acc[1] = {0.0};
-  for (int q = tid; q < m.nplanes; q += TX * TY) acc[0] += ((volatile double*)partials)[q];
+  double acc[1] = {strided_sum(partials, nplanes + (int)gridDim.x)};
   block_sum<1>(acc, sh);
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     st->pw = acc[0];
     st->alpha = st->eta / (acc[0] != 0.0 ? acc[0] : INFINITY);
     st->counter = 0u;
@@ -1311,23 +1388,36 @@ template <typename T>
 int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* pdot, int alpd,
                     int do_dot, const T* pa_val, const T* pv_val, const T* pr_val) {
   const Meta& m = ctx->meta;
+  const long long nc = ctx->lay.ncell;
   const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
-  k_mvA<T><<<gA, blk, 0, ctx->stream>>>(
-      m, in, vcm, tp<unsigned int>(ctx, PYIB_T_PA_BITS), tp<int>(ctx, PYIB_T_PA_ROW),
-      tp<long long>(ctx, PYIB_T_PA_PTR), tp<int>(ctx, PYIB_T_PA_COL), pa_val, ctx->nA, ctx->st);
+  k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, pa_val, ctx->nA,
+                                        ctx->st);
   CKL();
+  if (ctx->nA > 0) {
+    k_patchA<T><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
+        ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR), tp<int>(ctx, PYIB_T_PA_COL),
+        pa_val, in, vcm, nc, ctx->st);
+    CKL();
+  }
   const T* vsrc = vcm;
   if (alpd) {
-    k_mvV<T><<<gA, blk, 0, ctx->stream>>>(
-        m, vcm, vq, tp<unsigned int>(ctx, PYIB_T_PV_BITS), tp<int>(ctx, PYIB_T_PV_ROW),
-        tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL), pv_val, ctx->st);
+    k_mvV<T><<<gA, blk, 0, ctx->stream>>>(m, vcm, vq, nullptr, nullptr, nullptr, nullptr, pv_val, ctx->st);
     CKL();
+    if (ctx->nV > 0) {
+      k_patchV<T><<<patch_grid(3 * ctx->nV), kThreads, 0, ctx->stream>>>(
+          ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL),
+          pv_val, vcm, vq, nc, ctx->st);
+      CKL();
+    }
     vsrc = vq;
   }
   k_mvRI<T><<<gR, blk, 0, ctx->stream>>>(
-      m, vsrc, out, pdot, tp<unsigned int>(ctx, PYIB_T_PR_BITS), tp<int>(ctx, PYIB_T_PR_ROW),
-      tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL), pr_val, ctx->partials, ctx->st,
-      do_dot);
+      m, vsrc, out, pdot, tp<unsigned int>(ctx, PYIB_T_PR_BITS), nullptr, nullptr, nullptr, pr_val,
+      ctx->partials, ctx->st, do_dot);
+  CKL();
+  k_patchRI<T><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
+      ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL),
+      pr_val, vsrc, out, pdot, ctx->partials, m.nplanes, ctx->st, do_dot);
   CKL();
   return PYIB_OK;
 }
@@ -2020,6 +2110,9 @@ int pyib_finalize(pyib_ctx* ctx, const int64_t* counts, int32_t ncounts) {
   ctx->nA = counts[0];
   ctx->nV = counts[1];
   ctx->nR = counts[2];
+  if ((long long)ctx->meta.gxR * ctx->meta.gyR * ctx->meta.gzR + patch_grid(ctx->nR) > kPartStride ||
+      (long long)ctx->meta.nplanes + patch_grid(ctx->nR) > kPartStride)
+    return set_err(ctx, PYIB_E_ARG, "too many reduction slots for this layout");
   if (ctx->n_bf != ctx->lay.nbface)
     return set_err(ctx, PYIB_E_ARG, "boundary face table has %lld rows, layout says %d", ctx->n_bf,
                    ctx->lay.nbface);
@@ -2293,7 +2386,44 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
   CK(cudaEventSynchronize(ctx->ev1));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  *ms_per = ms / reps;
+  ms_per[0] = ms / reps;
+  // each kernel of the matvec alone, same inputs (run after a full matvec, so every
+  // intermediate it reads is current)
+  const Meta& m = ctx->meta;
+  const long long nc = ctx->lay.ncell;
+  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
+  for (int kern = 0; kern < 6; ++kern) {
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int q = 0; q < reps; ++q) {
+      switch (kern) {
+        case 0: k_mvA<double><<<gA, blk, 0, ctx->stream>>>(m, ctx->work_e, ctx->vcm, nullptr, nullptr, nullptr,
+                                                           nullptr, nullptr, ctx->nA, ctx->st); break;
+        case 1: k_patchA<double><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
+                    ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR),
+                    tp<int>(ctx, PYIB_T_PA_COL), tp<double>(ctx, PYIB_T_PA_VAL), ctx->work_e, ctx->vcm, nc,
+                    ctx->st); break;
+        case 2: k_mvV<double><<<gA, blk, 0, ctx->stream>>>(m, ctx->vcm, ctx->vq, nullptr, nullptr, nullptr,
+                                                           nullptr, nullptr, ctx->st); break;
+        case 3: k_patchV<double><<<patch_grid(3 * ctx->nV), kThreads, 0, ctx->stream>>>(
+                    ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR),
+                    tp<int>(ctx, PYIB_T_PV_COL), tp<double>(ctx, PYIB_T_PV_VAL), ctx->vcm, ctx->vq, nc,
+                    ctx->st); break;
+        case 4: k_mvRI<double><<<gR, blk, 0, ctx->stream>>>(m, ctx->vq, ctx->work_e2, ctx->work_e,
+                                                            tp<unsigned int>(ctx, PYIB_T_PR_BITS), nullptr,
+                                                            nullptr, nullptr, nullptr, ctx->partials, ctx->st,
+                                                            1); break;
+        default: k_patchRI<double><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
+                    ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR),
+                    tp<int>(ctx, PYIB_T_PR_COL), tp<double>(ctx, PYIB_T_PR_VAL), ctx->vq, ctx->work_e2,
+                    ctx->work_e, ctx->partials, m.nplanes, ctx->st, 1); break;
+      }
+      CKL();
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ms_per[1 + kern] = ms / reps;
+  }
   return PYIB_OK;
 }
 

@@ -175,6 +175,7 @@ class DeviceSolver:
             mask[rows_p] = True
             ptr, col, val = _csr_arrays(M)
             h.upload(tag + "_BITS", _bits(mask))
+            h.upload(tag + "_IDS", np.asarray(rows_p, dtype=np.int32))
             h.upload(tag + "_ROW", _rowmap(n, rows_p))
             h.upload(tag + "_PTR", ptr)
             h.upload(tag + "_COL", col)

@@ -116,6 +116,7 @@ enum pyib_table {
   PYIB_T_LC_CPOS,                                        /* f64[ncell*3] cell centres   */
   PYIB_T_PREC_BITS,         /* u32 bitmask: edges whose PREC differs from their level's value */
   PYIB_T_PREC_REG,          /* f64[nlevels] PREC of a level's regular edges              */
+  PYIB_T_PA_IDS, PYIB_T_PV_IDS, PYIB_T_PR_IDS, /* i32 dense ids of the patch rows (A, V, RI) */
   PYIB_T_COUNT
 };
 
@@ -218,7 +219,10 @@ int pyib_cg_timing(pyib_ctx* ctx, double* out, int32_t reset);
  * the end, waits for it and returns the elapsed milliseconds. */
 int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms);
 /* Times reps back-to-back matvecs (WORK_E -> WORK_E2, viscous block) with CUDA
- * events; *ms_per = milliseconds per matvec (benchmark support). */
+ * events (benchmark support).  ms_per holds 7 doubles: [0] one matvec, then one
+ * launch of each of its kernels alone: [1] curl+interp template, [2] its patch
+ * rows, [3] viscous template, [4] its patch rows, [5] integr+rot template with the
+ * dot, [6] its patch rows with the final reduction. */
 int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
 
 /* Deterministic spreading that allocates nothing.  No counterpart in the reference.
