@@ -383,7 +383,7 @@ def main():
     ap.add_argument("--workload", default="d32_oscillating_sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="float64", choices=["float64", "mixed"])
-    ap.add_argument("--mixed-tol", type=float, default=1e-4)
+    ap.add_argument("--mixed-tol", type=float, default=0.1)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

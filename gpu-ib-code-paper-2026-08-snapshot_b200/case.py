@@ -146,7 +146,7 @@ def validate_config(raw: dict) -> dict:
         raise CaseConfigError("runtime.device must be 'b200' here ('cpu'/'cuda' are the reference's backends)")
     if rt["precision"] not in {"float64", "mixed"}:
         raise CaseConfigError("runtime.precision must be 'float64' or 'mixed'")
-    rt["mixed_tolerance"] = _positive("runtime.mixed_tolerance", rt.get("mixed_tolerance", 1e-4))
+    rt["mixed_tolerance"] = _positive("runtime.mixed_tolerance", rt.get("mixed_tolerance", 0.1))
     mesh = cfg["mesh"]
     mk = str(mesh["kind"])
     if mk not in {"uniform_box", "sphere_concentric", "sphere_wake", "nested_boxes"}:

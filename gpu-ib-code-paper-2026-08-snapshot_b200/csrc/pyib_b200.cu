@@ -65,6 +65,7 @@ struct Meta {
 struct CGState {
   double eta, eta_new, pw, alpha, beta, thresh, l2_0, xnorm;
   double true_eta, true_l2, tol1, tol2;
+  double aux0, aux1;             // scalars of the mixed solver's flexible-CG outer loop
   double rou, kfac;              // V block: rou*v - kfac*(Vd v)
   double thresh_in;              // inner (float32) stop threshold of the mixed solver
   int m, done, iters, check, cg_max, alpd, stop, pad1;
@@ -102,6 +103,7 @@ struct pyib_ctx {
         *vq32 = nullptr, *prec32 = nullptr;
   float *pa_val32 = nullptr, *pv_val32 = nullptr, *pr_val32 = nullptr;
   double *diag1 = nullptr, *diag2 = nullptr;   // diag(R I P C) and diag(R I Vd' P C)
+  double *mix_q = nullptr;                      // previous A d of the flexible-CG outer loop
   double diag_for_kfac = -1.0, diag_for_rou = -1.0;
   bool diag_ready = false;
   cudaGraphExec_t mix_graph = nullptr;
@@ -882,6 +884,60 @@ __global__ void __launch_bounds__(kThreads) k_mix_resid(long long ne, double* r6
   }
 }
 
+// flexible CG outer loop (float64): aux0 = sum z.q_prev with z = the float32 inner solution
+__global__ void __launch_bounds__(kThreads) k_fcg_zq(long long ne, const float* __restrict__ z32,
+                                                     const double* __restrict__ qprev,
+                                                     const double* __restrict__ prec, double* partials,
+                                                     CGState* st) {
+  double v[1] = {0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x)
+    if (prec[e] != 0.0) v[0] += (double)z32[e] * qprev[e];
+  if (grid_sum<1>(v, partials, &st->counter)) st->aux0 = v[0];
+}
+
+// d = z - coef * d on unmasked edges (0 elsewhere)
+__global__ void k_fcg_dir(long long ne, const float* __restrict__ z32, double* d, double coef,
+                          const double* __restrict__ prec) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x)
+    d[e] = prec[e] != 0.0 ? (double)z32[e] - coef * d[e] : 0.0;
+}
+
+// aux1 = sum d.r
+__global__ void __launch_bounds__(kThreads) k_fcg_dr(long long ne, const double* __restrict__ d,
+                                                     const double* __restrict__ r, double* partials,
+                                                     CGState* st) {
+  double v[1] = {0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x)
+    v[0] += d[e] * r[e];
+  if (grid_sum<1>(v, partials, &st->counter)) st->aux1 = v[0];
+}
+
+// x += alpha d; r -= alpha q on unmasked edges; true_eta = sum (r*prec)*r, true_l2 = sum r^2
+__global__ void __launch_bounds__(kThreads) k_fcg_step(long long ne, const double* __restrict__ d,
+                                                       const double* __restrict__ q, double* x, double* r,
+                                                       const double* __restrict__ prec, double alpha,
+                                                       double* partials, CGState* st) {
+  double v[2] = {0.0, 0.0};
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double pr = prec[e];
+    x[e] += alpha * d[e];
+    if (pr != 0.0) {
+      const double re = r[e] - alpha * q[e];
+      r[e] = re;
+      v[0] += (re * pr) * re;
+      v[1] += re * re;
+    }
+  }
+  if (grid_sum<2>(v, partials, &st->counter)) {
+    st->true_eta = v[0];
+    st->true_l2 = v[1];
+  }
+}
+
 // diagonal probing: p = 1 on the edges of one colour (level L, axis a, index residues mod q)
 __global__ void k_probe_set(long long ne, long long base, int dx, int dy, int cnt, int q, int ci, int cj,
                             int ck, double* p, int clear) {
@@ -1629,6 +1685,7 @@ int ensure_mixed(pyib_ctx* ctx) {
   RET(alloc(ctx, (void**)&ctx->vq32, 3 * nc * sizeof(float)));
   RET(alloc(ctx, (void**)&ctx->diag1, ne * sizeof(double)));
   RET(alloc(ctx, (void**)&ctx->diag2, ne * sizeof(double)));
+  RET(alloc(ctx, (void**)&ctx->mix_q, ne * sizeof(double)));
   const int tabs[3] = {PYIB_T_PA_VAL, PYIB_T_PV_VAL, PYIB_T_PR_VAL};
   float** outs[3] = {&ctx->pa_val32, &ctx->pv_val32, &ctx->pr_val32};
   for (int q = 0; q < 3; ++q) {
@@ -1719,8 +1776,9 @@ int clear_done(pyib_ctx* ctx) {
   return PYIB_OK;
 }
 
-// Mixed precision: the float64 stopping test of helm_solve on the true residual,
-// reached by float32 PCG corrections (Jacobi on diag(A)) and float64 residual updates.
+// Mixed precision: the float64 stopping test of helm_solve on the float64 residual,
+// reached by float32 PCG inner solves (Jacobi on diag(A)) combined by a float64
+// flexible-CG outer loop.
 int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
@@ -1748,12 +1806,21 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   int inner_total = 0, sweeps = 0;
   const double eps2 = ctx->prm.mixed_tol * ctx->prm.mixed_tol;
   const int max_sweeps = ctx->prm.mixed_max_sweeps > 0 ? ctx->prm.mixed_max_sweeps : 40;
+  // Flexible CG (one previous direction) in float64 around float32 inner solves:
+  //   z = inner(r);  d = z - (z.q_prev / d_prev.q_prev) d_prev;  q = A d;
+  //   alpha = d.r / d.q;  x += alpha d;  r -= alpha q
+  // r stays the float64 residual of the reference's criterion, updated with exact
+  // float64 products, so the stopping test is the float64 one.
+  double* d = ctx->p;                 // direction (k_cg_init's p is not used here)
+  double* q = ctx->w;                 // A d
+  double* qprev = ctx->mix_q;
+  double dq_prev = 0.0;
   while (!(eta < thresh) && sweeps < max_sweeps) {
     k_mix_start<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
                                                             ctx->p32, eps2, ctx->partials, ctx->st);
     CKL();
     const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
-    for (long long q = 0; q < max_chunks; ++q) {
+    for (long long c = 0; c < max_chunks; ++c) {
       CK(cudaGraphLaunch(ctx->mix_graph, ctx->stream));
       ctx->launches += 5LL * ctx->prm.check;
       CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1761,16 +1828,33 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
       if (ctx->st_host->done) break;
     }
     inner_total += ctx->st_host->iters;
-    k_mix_apply<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, ctx->work_e2, ctx->x);
+    double coef = 0.0;
+    if (sweeps > 0 && dq_prev != 0.0) {
+      k_fcg_zq<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, qprev, prec, ctx->partials, ctx->st);
+      CKL();
+      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      coef = ctx->st_host->aux0 / dq_prev;
+    }
+    k_fcg_dir<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, d, coef, prec);
     CKL();
     RET(clear_done(ctx));
-    RET(launch_matvec(ctx, ctx->work_e2, ctx->w, 1, 0));
-    k_mix_resid<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->w, prec, ctx->partials, ctx->st);
+    RET(launch_matvec(ctx, d, q, 1, 1));          // q = A d, st->pw = d.q
+    k_fcg_dr<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, ctx->r, ctx->partials, ctx->st);
+    CKL();
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double dq = ctx->st_host->pw, dr = ctx->st_host->aux1;
+    if (!(dq > 0.0) || !std::isfinite(dr)) break;
+    k_fcg_step<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, q, ctx->x, ctx->r, prec, dr / dq,
+                                                           ctx->partials, ctx->st);
     CKL();
     CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     eta = ctx->st_host->true_eta;
     l2 = ctx->st_host->true_l2;
+    std::swap(q, qprev);             // local swap: the captured graphs keep ctx->w
+    dq_prev = dq;
     ++sweeps;
     if (!std::isfinite(eta)) break;
   }
@@ -2052,7 +2136,7 @@ int pyib_destroy(pyib_ctx* ctx) {
                   ctx->ibcell, ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
                   ctx->sort_vals_out, ctx->sort_tmp, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
                   ctx->vcm32, ctx->vq32, ctx->prec32, ctx->pa_val32, ctx->pv_val32,
-                  ctx->pr_val32, ctx->diag1, ctx->diag2};
+                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->mix_q};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);

@@ -58,7 +58,7 @@ class DeviceSolver:
 
     def __init__(self, lay: NestedLayout, *, rou, visc, cavity, cg_check_interval=20,
                  cg_max_iterations=1000, strict=False, ac=0.5, ad=0.5, tol1=1e-10, tol2=1e-9,
-                 device=0, precision="float64", mixed_tol=1e-4, mixed_max_sweeps=40):
+                 device=0, precision="float64", mixed_tol=0.1, mixed_max_sweeps=200):
         if not getattr(lay, "_built", False):
             lay.build()
         self.lay = lay

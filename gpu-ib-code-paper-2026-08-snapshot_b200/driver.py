@@ -48,7 +48,7 @@ class B200Driver:
 
     def __init__(self, layout: NestedLayout, visc, rou=1.0, ac=0.5, ad=0.5, *,
                  cg_max_iterations=1000, fail_on_cg_nonconvergence=False, device=0,
-                 precision="float64", mixed_tol=1e-4):
+                 precision="float64", mixed_tol=0.1):
         if precision not in ("float64", "mixed"):
             raise ValueError("precision must be 'float64' or 'mixed'")
         self.precision = precision

@@ -71,7 +71,7 @@ class SphereRun:
     """One sphere case on one GPU: driver, markers, loads and the current state."""
 
     def __init__(self, case: SphereCase, device=0, layout=None, check_interval=20,
-                 precision="float64", mixed_tol=1e-4):
+                 precision="float64", mixed_tol=0.1):
         self.case = case
         lay = layout if layout is not None else case.layout()
         drv = B200Driver(lay, case.viscosity, case.density,

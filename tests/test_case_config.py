@@ -21,7 +21,7 @@ def test_defaults_and_normalisation():
     cfg = CS.validate_config(SMOKE)
     assert cfg["solver"]["cg_check_interval"] == 20
     assert cfg["ib"]["motion"]["axis"] == [0.0, 1.0, 0.0]
-    assert cfg["runtime"]["mixed_tolerance"] == pytest.approx(1e-4)
+    assert cfg["runtime"]["mixed_tolerance"] == pytest.approx(0.1)
 
 
 @pytest.mark.parametrize("patch, msg", [
