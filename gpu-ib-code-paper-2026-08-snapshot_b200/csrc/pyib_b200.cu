@@ -108,6 +108,7 @@ struct pyib_ctx {
   bool diag_ready = false;
   cudaGraphExec_t mix_graph = nullptr;
   int mix_graph_check = 0;
+  long long mix_graph_kernels = 0;   // kernel nodes in mix_graph
   // reduction / state
   double* partials = nullptr;
   CGState* st = nullptr;
@@ -129,6 +130,7 @@ struct pyib_ctx {
   // graphs
   cudaGraphExec_t cg_graph = nullptr;
   int cg_graph_check = 0;
+  long long cg_graph_kernels = 0;    // kernel nodes in cg_graph
   int cg_graph_alpd = -1;
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
@@ -853,37 +855,6 @@ __global__ void __launch_bounds__(kThreads) k_cg_p32(long long ne, const float* 
     p32[e] = r32[e] * dinv[e] + beta * p32[e];
 }
 
-// correction: d64 = d32, x += d64
-__global__ void k_mix_apply(long long ne, const float* __restrict__ d32, double* d64, double* x) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x) {
-    const double d = (double)d32[e];
-    d64[e] = d;
-    x[e] += d;
-  }
-}
-
-// r64 -= A d (masked); eta = sum (r*prec)*r with the float64 criterion's preconditioner
-__global__ void __launch_bounds__(kThreads) k_mix_resid(long long ne, double* r64,
-                                                        const double* __restrict__ Ad,
-                                                        const double* __restrict__ prec,
-                                                        double* partials, CGState* st) {
-  double v[2] = {0.0, 0.0};
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x) {
-    const double pr = prec[e];
-    if (pr == 0.0) continue;
-    const double re = r64[e] - Ad[e];
-    r64[e] = re;
-    v[0] += (re * pr) * re;
-    v[1] += re * re;
-  }
-  if (grid_sum<2>(v, partials, &st->counter)) {
-    st->true_eta = v[0];
-    st->true_l2 = v[1];
-  }
-}
-
 // flexible CG outer loop (float64): aux0 = sum z.q_prev with z = the float32 inner solution
 __global__ void __launch_bounds__(kThreads) k_fcg_zq(long long ne, const float* __restrict__ z32,
                                                      const double* __restrict__ qprev,
@@ -1369,7 +1340,7 @@ int check_dev_err(pyib_ctx* ctx) {
 
 bool tables_ready(pyib_ctx* c) {
   const int need[] = {PYIB_T_PREC, PYIB_T_PREC_BITS, PYIB_T_PREC_REG, PYIB_T_CURL_PTR, PYIB_T_ROT_PTR, PYIB_T_P_PTR, PYIB_T_I_PTR,
-                      PYIB_T_CF_PTR, PYIB_T_F_LO, PYIB_T_F_HI, PYIB_T_F_AOL, PYIB_T_VOLCI};
+                      PYIB_T_CF_PTR, PYIB_T_F_LO, PYIB_T_F_HI, PYIB_T_F_AOL, PYIB_T_VOLCI, PYIB_T_PR_BITS};
   for (int t : need)
     if (!c->tab[t].ptr) return false;
   return true;
@@ -1572,6 +1543,20 @@ int cg_iteration(pyib_ctx* ctx) {
   return PYIB_OK;
 }
 
+// kernel nodes of a captured graph (the launch count of one replay)
+long long graph_kernels(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+  long long k = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
 int build_cg_graph(pyib_ctx* ctx) {
   if (ctx->cg_graph && ctx->cg_graph_check == ctx->prm.check) return PYIB_OK;
   if (ctx->cg_graph) {
@@ -1579,12 +1564,15 @@ int build_cg_graph(pyib_ctx* ctx) {
     ctx->cg_graph = nullptr;
   }
   cudaGraph_t g;
+  const long long launched = ctx->launches;   // captured launches are counted per replay instead
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   int rc = PYIB_OK;
   for (int q = 0; q < ctx->prm.check && rc == PYIB_OK; ++q) rc = cg_iteration(ctx);
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->launches = launched;
   if (rc != PYIB_OK) return rc;
   if (e != cudaSuccess) return set_err(ctx, PYIB_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  ctx->cg_graph_kernels = graph_kernels(g);
   e = cudaGraphInstantiate(&ctx->cg_graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_err(ctx, PYIB_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
@@ -1611,7 +1599,7 @@ int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
     const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
     for (long long q = 0; q < max_chunks; ++q) {
       CK(cudaGraphLaunch(ctx->cg_graph, ctx->stream));
-      ctx->launches += 5LL * ctx->prm.check;
+      ctx->launches += ctx->cg_graph_kernels;
       CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
       if (ctx->st_host->done) break;
@@ -1757,12 +1745,15 @@ int build_mix_graph(pyib_ctx* ctx) {
     ctx->mix_graph = nullptr;
   }
   cudaGraph_t g;
+  const long long launched = ctx->launches;   // captured launches are counted per replay instead
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   int rc = PYIB_OK;
   for (int q = 0; q < ctx->prm.check && rc == PYIB_OK; ++q) rc = mix_iteration(ctx);
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->launches = launched;
   if (rc != PYIB_OK) return rc;
   if (e != cudaSuccess) return set_err(ctx, PYIB_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  ctx->mix_graph_kernels = graph_kernels(g);
   e = cudaGraphInstantiate(&ctx->mix_graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_err(ctx, PYIB_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
@@ -1822,7 +1813,7 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
     const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
     for (long long c = 0; c < max_chunks; ++c) {
       CK(cudaGraphLaunch(ctx->mix_graph, ctx->stream));
-      ctx->launches += 5LL * ctx->prm.check;
+      ctx->launches += ctx->mix_graph_kernels;
       CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
       if (ctx->st_host->done) break;
