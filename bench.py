@@ -390,6 +390,121 @@ def run_b200(args, world, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Mixed precision against float64 on the same case
+# ---------------------------------------------------------------------------
+def run_precision_compare(args, world, rank, local):
+    """Steps/s of the float64 and mixed forms and the mixed form's errors against float64.
+
+    Both forms start from the same state and advance warmup + steps steps; the
+    timings are CUDA events over the last ``steps`` steps, the errors are
+    relative l2 norms of the final fields (stream function s, face flux U = curl s,
+    cell velocity vc, marker forces fL, Eulerian force fE) and of the body-force
+    history over all steps.
+    """
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    from pyib_b200 import build
+    from pyib_b200.cases import CASES
+    from pyib_b200.device import LayoutTables
+    from pyib_b200.runner import SphereRun
+
+    build.build_library()
+    if world > 1:
+        raise SystemExit("the precision comparison runs on one GPU")
+    case = CASES[args.workload]
+    tables = LayoutTables(case.layout().build(), case.cavity)
+    out = {}
+    for prec in ("float64", "mixed"):
+        run = SphereRun(case, device=0, tables=tables, precision=prec, mixed_tol=args.mixed_tol)
+        sv = run.drv.solver
+        forces = []
+        for _ in range(args.warmup):
+            forces.append(run.advance()["body_force"].copy())
+        ev = C.c_double(0.0)
+        sv.h.call("pyib_event", 0, None)
+        its = 0
+        for _ in range(args.steps):
+            forces.append(run.advance()["body_force"].copy())
+            its += run.drv.helmholtz_total_iterations_last_step
+        sv.h.call("pyib_event", 1, C.byref(ev))
+        sv.h.call("pyib_calc_vel")
+        out[prec] = dict(seconds=ev.value / 1000.0, iterations=its, s=np.asarray(run.s).copy(),
+                         U=sv.get("U"), vc=np.asarray(run.vc).copy(), fL=np.asarray(run.drv.ib_force_L).copy(),
+                         fE=np.asarray(run.drv.ib_force_E).copy(), force=np.array(forces))
+        sv.h.close()
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    f64, mix = out["float64"], out["mixed"]
+    line = {
+        "metric": "mixed vs float64 steps/s and errors", "workload": case.name,
+        "steps": args.steps, "warmup": args.warmup, "mixed_tolerance": args.mixed_tol,
+        "float64": {"steps_per_s": args.steps / f64["seconds"], "cg_iterations": f64["iterations"]},
+        "mixed": {"steps_per_s": args.steps / mix["seconds"], "inner_iterations": mix["iterations"]},
+        "errors_vs_float64": {k: rel(mix[k], f64[k]) for k in ("s", "U", "vc", "fL", "fE", "force")},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Batched sweep: independent cases of uneven size, concurrent vs one at a time
+# ---------------------------------------------------------------------------
+def run_batch(args, world, rank, local):
+    """Aggregate cell-updates/s of the seeded sweep, concurrently and one case at a time.
+
+    Both timings advance every case by ``--steps`` steps (consecutive steps of the
+    same runs: first concurrently, then sequentially); host wall clock around
+    each phase, every case's last call having waited for its own stream.
+    """
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    from pyib_b200 import build
+    from pyib_b200.batch import BatchRun, sweep_cases
+
+    build.build_library()
+    if world > 1:
+        raise SystemExit("the batched sweep runs on one GPU")
+    cases = sweep_cases(args.batch_cases, seed=0)
+    t_setup = time.perf_counter()
+    batch = BatchRun(cases, device=0, precision=args.precision, mixed_tol=args.mixed_tol)
+    batch.tune()
+    setup_s = time.perf_counter() - t_setup
+    cells = batch.cells
+    for _ in range(args.warmup):
+        batch.advance(1, concurrent=True)
+    sampler = ClockSampler(0)
+    sampler.start()
+    t_con, st_con = batch.advance(args.steps, concurrent=True)
+    t_seq, st_seq = batch.advance(args.steps, concurrent=False)
+    clocks = sampler.stop()
+    upd = float(sum(cells)) * args.steps
+    launches = 0
+    timing = (C.c_double * 5)()
+    for r in batch.runs:
+        r.drv.solver.h.call("pyib_cg_timing", timing, 0)
+        launches += int(timing[2])
+    line = {
+        "metric": "batched sweep cell-updates/s", "value": upd / t_con, "unit": "cell-updates/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_con / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "float64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": "batched_sweep", "cases": len(cases), "seed": 0,
+                   "cells_per_diameter_histogram": batch.histogram(), "total_cells": int(sum(cells)),
+                   "levels": 2, "precision": args.precision, "setup_seconds": setup_s,
+                   "l2": "inputs larger than L2"},
+        "concurrent": {"seconds": t_con, **st_con},
+        "one_at_a_time": {"value": upd / t_seq, "seconds": t_seq, **st_seq},
+        "gpu_launches_since_setup": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -400,10 +515,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="float64", choices=["float64", "mixed"])
     ap.add_argument("--mixed-tol", type=float, default=0.1)
+    ap.add_argument("--batch-cases", type=int, default=64)
+    ap.add_argument("--compare-precision", action="store_true",
+                    help="run the workload in float64 and mixed precision and report the errors")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     world, rank, local = dist_env()
+    if args.workload == "batched_sweep":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched sweep has no reference "
+                              "counterpart (the reference runs one case per process)"}), flush=True)
+            return 0
+        return run_batch(args, world, rank, local)
+    if args.compare_precision:
+        return run_precision_compare(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     return run_b200(args, world, rank, local)

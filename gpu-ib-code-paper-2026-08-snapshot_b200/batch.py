@@ -1,0 +1,120 @@
+"""Batched sweep: many independent oscillating-sphere cases of uneven size on one GPU.
+
+Each case is a full ``SphereRun`` (its own library context, CUDA stream, CG
+graphs and autotuned tiles).  ``BatchRun.advance`` drives every case from its
+own host thread -- one context per host thread, as the C ABI requires -- so the
+cases' graph replays and kernels run concurrently on their streams and fill
+the gaps a single case leaves (host polls every ``check`` iterations, the tail
+blocks of small grids, launch latency of the patch kernels).  The library
+calls release the Python interpreter lock (ctypes), so the threads overlap.
+
+Cases with the same resolution share one ``LayoutTables`` (operators, masks,
+patch rows), built once on the host.
+
+The sweep draw follows the batched configuration: seeded
+``numpy.random.default_rng(seed)``; per case, in this order, ``D`` cells per
+diameter from {12, 16, 20, 24, 32}, amplitude ``A/D`` uniform in [0.05, 0.3],
+``Re0`` log-uniform in [0.1, 10]; two nested levels (half widths 2D and 4D),
+closed no-slip walls, omega = 3.6, 200 steps per period.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from collections import Counter
+
+import numpy as np
+
+from .cases import SphereCase
+from .device import LayoutTables
+from .runner import SphereRun
+
+SWEEP_CELLS_PER_DIAMETER = (12, 16, 20, 24, 32)
+
+
+def sweep_cases(count=64, seed=0, cg_max_iterations=20000):
+    """The seeded sweep: ``count`` cases drawn as described in the module docstring."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(int(count)):
+        d = int(rng.choice(SWEEP_CELLS_PER_DIAMETER))
+        a = float(rng.uniform(0.05, 0.3))
+        re0 = float(10.0 ** rng.uniform(-1.0, 1.0))
+        out.append(SphereCase(name=f"sweep_{i:02d}_d{d}", cells_per_diameter=d, half_widths_d=(2.0, 4.0),
+                              reynolds=re0, amplitude_d=a, cg_max_iterations=cg_max_iterations))
+    return out
+
+
+class BatchRun:
+    """Independent sphere cases on one GPU, stepped concurrently or one at a time."""
+
+    def __init__(self, cases, device=0, precision="float64", mixed_tol=0.1):
+        self.cases = list(cases)
+        self.tables = {}
+        self.runs = []
+        for c in self.cases:
+            key = (c.cells_per_diameter, tuple(c.half_widths_d), bool(c.cavity))
+            if key not in self.tables:
+                self.tables[key] = LayoutTables(c.layout().build(), c.cavity)
+            self.runs.append(SphereRun(c, device=device, tables=self.tables[key], precision=precision,
+                                       mixed_tol=mixed_tol))
+
+    @property
+    def cells(self):
+        """Existing cells of every case (the unit of cell-updates/s)."""
+        return [int(r.drv.layout.cell_active.sum()) for r in self.runs]
+
+    def histogram(self):
+        return dict(sorted(Counter(c.cells_per_diameter for c in self.cases).items()))
+
+    def tune(self):
+        """Run each context's matvec autotuner alone, before any concurrent work."""
+        import ctypes as C
+        ms = (C.c_double * 7)()
+        for r in self.runs:
+            sv = r.drv.solver
+            sv.set("WORK_E", np.zeros(sv.lay.NE))
+            sv.h.call("pyib_bench_matvec", 1, C.c_double(r.dt), ms)
+
+    def _stats(self, per_run_iters):
+        return {"cg_iterations": int(sum(sum(x) for x in per_run_iters)),
+                "max_case_iterations": int(max(sum(x) for x in per_run_iters))}
+
+    def advance(self, steps=1, concurrent=True):
+        """Advance every case by ``steps`` steps; returns (seconds, stats)."""
+        iters = [[] for _ in self.runs]
+        errors = []
+
+        def work(q):
+            r = self.runs[q]
+            try:
+                for _ in range(steps):
+                    r.advance()
+                    iters[q].append(r.drv.helmholtz_total_iterations_last_step)
+            except BaseException as exc:       # re-raised on the calling thread
+                errors.append((q, exc))
+
+        t0 = time.perf_counter()
+        if concurrent:
+            threads = [threading.Thread(target=work, args=(q,), daemon=True) for q in range(len(self.runs))]
+            for t in threads:
+                t.start()
+            for t in threads:
+                t.join()
+        else:
+            for q in range(len(self.runs)):
+                work(q)
+                if errors:
+                    break
+        seconds = time.perf_counter() - t0
+        if errors:
+            q, exc = errors[0]
+            raise RuntimeError(f"case {self.cases[q].name} failed: {exc}") from exc
+        return seconds, self._stats(iters)
+
+    def close(self):
+        """Release every case's device context."""
+        for r in self.runs:
+            if r.drv._solver is not None:
+                r.drv._solver.h.close()
+        self.runs = []

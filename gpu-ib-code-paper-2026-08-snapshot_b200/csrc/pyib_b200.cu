@@ -65,7 +65,6 @@ struct Meta {
 struct CGState {
   double eta, eta_new, pw, alpha, beta, thresh, l2_0, xnorm;
   double true_eta, true_l2, tol1, tol2;
-  double aux0, aux1;             // scalars of the mixed solver's flexible-CG outer loop
   double rou, kfac;              // V block: rou*v - kfac*(Vd v)
   double thresh_in;              // inner (float32) stop threshold of the mixed solver
   int m, done, iters, check, cg_max, alpd, stop, pad1;
@@ -103,7 +102,6 @@ struct pyib_ctx {
         *vq32 = nullptr, *prec32 = nullptr;
   float *pa_val32 = nullptr, *pv_val32 = nullptr, *pr_val32 = nullptr;
   double *diag1 = nullptr, *diag2 = nullptr;   // diag(R I P C) and diag(R I Vd' P C)
-  double *mix_q = nullptr;                      // previous A d of the flexible-CG outer loop
   double diag_for_kfac = -1.0, diag_for_rou = -1.0;
   bool diag_ready = false;
   cudaGraphExec_t mix_graph = nullptr;
@@ -594,9 +592,9 @@ __global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __
   vq[d * nc + c] = (T)st->rou * vd[c] - (T)st->kfac * csr_row<T>(ptr, col, val, vd, r);
 }
 
-// w rows (columns index the component-major vq), plus their share of p.w; the last
-// block sums the per-plane partials of k_mvRI and this kernel's per-block partials
-// in a fixed order and sets alpha = eta / p.w.
+// w rows (columns index the component-major vq), plus their share of p.w; the
+// per-plane partials of k_mvRI and the rows' shares are summed in a fixed order
+// (independent of the z-chunk depth) and the last block sets alpha = eta / p.w.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* __restrict__ ids,
                                                       const long long* __restrict__ ptr,
@@ -613,18 +611,24 @@ __global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* _
     if (do_dot) dot[0] = (double)p[e] * (double)acc;
   }
   if (!do_dot) return;
-  __shared__ double sh[32];
+  __shared__ double sh[2 * 32];
   __shared__ bool last;
-  block_sum<1>(dot, sh);
+  // Two-stage fixed-order sum: each block adds a fixed slice of k_mvRI's per-plane
+  // partials to its own rows' share, and the last block sums one value per block.
+  const int per = (nplanes + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int q0 = min(nplanes, (int)blockIdx.x * per), q1 = min(nplanes, q0 + per);
+  double v2[2] = {dot[0], 0.0};
+  for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) v2[1] += partials[q];
+  block_sum<2>(v2, sh);
   if (threadIdx.x == 0) {
-    partials[nplanes + blockIdx.x] = dot[0];
+    partials[nplanes + blockIdx.x] = v2[0] + v2[1];
     __threadfence();
     last = atomicAdd(&st->counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
-  double acc[1] = {strided_sum(partials, nplanes + (int)gridDim.x)};
+  double acc[1] = {strided_sum(partials + nplanes, (int)gridDim.x)};
   block_sum<1>(acc, sh);
   if (threadIdx.x == 0) {
     st->pw = acc[0];
@@ -855,49 +859,53 @@ __global__ void __launch_bounds__(kThreads) k_cg_p32(long long ne, const float* 
     p32[e] = r32[e] * dinv[e] + beta * p32[e];
 }
 
-// flexible CG outer loop (float64): aux0 = sum z.q_prev with z = the float32 inner solution
-__global__ void __launch_bounds__(kThreads) k_fcg_zq(long long ne, const float* __restrict__ z32,
-                                                     const double* __restrict__ qprev,
-                                                     const double* __restrict__ prec, double* partials,
-                                                     CGState* st) {
+// Reliable update of the float32 CG: r32 = float(r64) (the float64 residual after
+// folding the float32 correction into x), correction reset, eta from the new residual,
+// beta = eta_new / eta_old so that k_cg_p32 continues the same search direction.
+__global__ void __launch_bounds__(kThreads) k_mix_reliable(long long ne, const double* __restrict__ r64,
+                                                           const float* __restrict__ dinv, float* r32,
+                                                           float* d32, double eps_in2, double* partials,
+                                                           CGState* st) {
   double v[1] = {0.0};
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x)
-    if (prec[e] != 0.0) v[0] += (double)z32[e] * qprev[e];
-  if (grid_sum<1>(v, partials, &st->counter)) st->aux0 = v[0];
+       e += (long long)gridDim.x * blockDim.x) {
+    const float di = dinv[e];
+    const float re = di != 0.f ? (float)r64[e] : 0.f;
+    r32[e] = re;
+    d32[e] = 0.f;
+    v[0] += (double)(re * di) * (double)re;
+  }
+  if (grid_sum<1>(v, partials, &st->counter)) {
+    const double en = v[0];
+    st->beta = en / (st->eta != 0.0 ? st->eta : INFINITY);
+    st->eta = en;
+    st->thresh_in = eps_in2 * en;
+    st->m = 0;
+    st->iters = 0;
+    st->done = en > 0.0 && isfinite(en) ? 0 : 1;
+  }
 }
 
-// d = z - coef * d on unmasked edges (0 elsewhere)
-__global__ void k_fcg_dir(long long ne, const float* __restrict__ z32, double* d, double coef,
-                          const double* __restrict__ prec) {
+// d = double(x32) on unmasked edges (0 elsewhere): the float32 correction in float64
+__global__ void k_mix_widen(long long ne, const float* __restrict__ x32, double* d,
+                            const double* __restrict__ prec) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x)
-    d[e] = prec[e] != 0.0 ? (double)z32[e] - coef * d[e] : 0.0;
+    d[e] = prec[e] != 0.0 ? (double)x32[e] : 0.0;
 }
 
-// aux1 = sum d.r
-__global__ void __launch_bounds__(kThreads) k_fcg_dr(long long ne, const double* __restrict__ d,
-                                                     const double* __restrict__ r, double* partials,
-                                                     CGState* st) {
-  double v[1] = {0.0};
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x)
-    v[0] += d[e] * r[e];
-  if (grid_sum<1>(v, partials, &st->counter)) st->aux1 = v[0];
-}
-
-// x += alpha d; r -= alpha q on unmasked edges; true_eta = sum (r*prec)*r, true_l2 = sum r^2
-__global__ void __launch_bounds__(kThreads) k_fcg_step(long long ne, const double* __restrict__ d,
+// x += d; r -= q on unmasked edges; true_eta = sum (r*prec)*r, true_l2 = sum r^2
+__global__ void __launch_bounds__(kThreads) k_mix_fold(long long ne, const double* __restrict__ d,
                                                        const double* __restrict__ q, double* x, double* r,
-                                                       const double* __restrict__ prec, double alpha,
-                                                       double* partials, CGState* st) {
+                                                       const double* __restrict__ prec, double* partials,
+                                                       CGState* st) {
   double v[2] = {0.0, 0.0};
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
     const double pr = prec[e];
-    x[e] += alpha * d[e];
+    x[e] += d[e];
     if (pr != 0.0) {
-      const double re = r[e] - alpha * q[e];
+      const double re = r[e] - q[e];
       r[e] = re;
       v[0] += (re * pr) * re;
       v[1] += re * re;
@@ -1673,7 +1681,6 @@ int ensure_mixed(pyib_ctx* ctx) {
   RET(alloc(ctx, (void**)&ctx->vq32, 3 * nc * sizeof(float)));
   RET(alloc(ctx, (void**)&ctx->diag1, ne * sizeof(double)));
   RET(alloc(ctx, (void**)&ctx->diag2, ne * sizeof(double)));
-  RET(alloc(ctx, (void**)&ctx->mix_q, ne * sizeof(double)));
   const int tabs[3] = {PYIB_T_PA_VAL, PYIB_T_PV_VAL, PYIB_T_PR_VAL};
   float** outs[3] = {&ctx->pa_val32, &ctx->pv_val32, &ctx->pr_val32};
   for (int q = 0; q < 3; ++q) {
@@ -1768,8 +1775,7 @@ int clear_done(pyib_ctx* ctx) {
 }
 
 // Mixed precision: the float64 stopping test of helm_solve on the float64 residual,
-// reached by float32 PCG inner solves (Jacobi on diag(A)) combined by a float64
-// flexible-CG outer loop.
+// reached by one float32 PCG (Jacobi on diag(A)) with reliable float64 updates.
 int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
@@ -1797,20 +1803,18 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   int inner_total = 0, sweeps = 0;
   const double eps2 = ctx->prm.mixed_tol * ctx->prm.mixed_tol;
   const int max_sweeps = ctx->prm.mixed_max_sweeps > 0 ? ctx->prm.mixed_max_sweeps : 40;
-  // Flexible CG (one previous direction) in float64 around float32 inner solves:
-  //   z = inner(r);  d = z - (z.q_prev / d_prev.q_prev) d_prev;  q = A d;
-  //   alpha = d.r / d.q;  x += alpha d;  r -= alpha q
-  // r stays the float64 residual of the reference's criterion, updated with exact
-  // float64 products, so the stopping test is the float64 one.
-  double* d = ctx->p;                 // direction (k_cg_init's p is not used here)
+  // One float32 PCG (Jacobi on diag A) with reliable updates.  Whenever its residual
+  // has dropped by mixed_tol since the last update, the float32 correction is folded
+  // into x in float64 and r is recomputed in float64 (r -= A x32); the float32 CG then
+  // continues from the new residual with the same search direction (no restart), and
+  // the reference's float64 test on r decides when to stop.
+  double* d = ctx->p;                 // float64 copy of the float32 correction
   double* q = ctx->w;                 // A d
-  double* qprev = ctx->mix_q;
-  double dq_prev = 0.0;
+  k_mix_start<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
+                                                          ctx->p32, eps2, ctx->partials, ctx->st);
+  CKL();
+  const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
   while (!(eta < thresh) && sweeps < max_sweeps) {
-    k_mix_start<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
-                                                            ctx->p32, eps2, ctx->partials, ctx->st);
-    CKL();
-    const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
     for (long long c = 0; c < max_chunks; ++c) {
       CK(cudaGraphLaunch(ctx->mix_graph, ctx->stream));
       ctx->launches += ctx->mix_graph_kernels;
@@ -1819,35 +1823,25 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
       if (ctx->st_host->done) break;
     }
     inner_total += ctx->st_host->iters;
-    double coef = 0.0;
-    if (sweeps > 0 && dq_prev != 0.0) {
-      k_fcg_zq<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, qprev, prec, ctx->partials, ctx->st);
-      CKL();
-      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      coef = ctx->st_host->aux0 / dq_prev;
-    }
-    k_fcg_dir<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, d, coef, prec);
+    // x += x32, r -= A x32 in float64
+    k_mix_widen<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, d, prec);
     CKL();
     RET(clear_done(ctx));
-    RET(launch_matvec(ctx, d, q, 1, 1));          // q = A d, st->pw = d.q
-    k_fcg_dr<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, ctx->r, ctx->partials, ctx->st);
-    CKL();
-    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    const double dq = ctx->st_host->pw, dr = ctx->st_host->aux1;
-    if (!(dq > 0.0) || !std::isfinite(dr)) break;
-    k_fcg_step<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, q, ctx->x, ctx->r, prec, dr / dq,
-                                                           ctx->partials, ctx->st);
+    RET(launch_matvec(ctx, d, q, 1, 0));
+    k_mix_fold<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, q, ctx->x, ctx->r, prec, ctx->partials,
+                                                           ctx->st);
     CKL();
     CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     eta = ctx->st_host->true_eta;
     l2 = ctx->st_host->true_l2;
-    std::swap(q, qprev);             // local swap: the captured graphs keep ctx->w
-    dq_prev = dq;
     ++sweeps;
-    if (!std::isfinite(eta)) break;
+    if (!std::isfinite(eta) || eta < thresh) break;
+    k_mix_reliable<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
+                                                               eps2, ctx->partials, ctx->st);
+    CKL();
+    k_cg_p32<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r32, ctx->prec32, ctx->p32, ctx->st);
+    CKL();
   }
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   CK(cudaMemcpyAsync(ctx->s, ctx->x, ne * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -2127,7 +2121,7 @@ int pyib_destroy(pyib_ctx* ctx) {
                   ctx->ibcell, ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
                   ctx->sort_vals_out, ctx->sort_tmp, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
                   ctx->vcm32, ctx->vq32, ctx->prec32, ctx->pa_val32, ctx->pv_val32,
-                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->mix_q};
+                  ctx->pr_val32, ctx->diag1, ctx->diag2};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);

@@ -53,22 +53,126 @@ def _triplets_sorted(rows, cols, vals3, nrows):
     return np.cumsum(ptr), cols.astype(np.int32), np.ascontiguousarray(vals3, dtype=np.float64)
 
 
-class DeviceSolver:
-    """One GPU context holding a nested layout, its operators and the solver state."""
+class LayoutTables:
+    """Host-side tables of one layout and boundary kind, built once and shared.
 
-    def __init__(self, lay: NestedLayout, *, rou, visc, cavity, cg_check_interval=20,
-                 cg_max_iterations=1000, strict=False, ac=0.5, ad=0.5, tol1=1e-10, tol2=1e-9,
-                 device=0, precision="float64", mixed_tol=0.1, mixed_max_sweeps=200):
+    Everything a context uploads that depends only on the geometry (operators,
+    boundary masks, preconditioner, structured-matvec patches): several contexts
+    on the same nested layout -- the cases of a batched sweep with equal
+    resolution -- reuse one instance instead of rebuilding it per case.
+    """
+
+    def __init__(self, lay: NestedLayout, cavity):
         if not getattr(lay, "_built", False):
             lay.build()
         self.lay = lay
-        self.ops = ops = Operators(lay)
         self.cavity = bool(cavity)
+        self.ops = ops = Operators(lay)
         self.dir_mask = ops.dir_mask(self.cavity)
         self.inlet = ops.inlet_mask(self.cavity) & lay.edge_exists
         self.prec = ops.prec(self.dir_mask)
         self.plan = MatvecPlan(ops, self.dir_mask)
         self.bfaces = lay.boundary_faces()
+        self.arrays = {}
+        self._build()
+
+    def _build(self):
+        lay, ops, A = self.lay, self.ops, self.arrays
+        NC, NF, NE = lay.NC, lay.NF, lay.NE
+        A["PREC"] = self.prec
+        # per level, the value of the regular edges; edges that differ are flagged
+        reg = np.zeros(lay.N)
+        irregular = np.zeros(NE, dtype=bool)
+        for lv in lay.levels:
+            lo_e = lay.edge_base[lv.L][0]
+            hi_e = lay.edge_base[lv.L][2] + int(np.prod(lv.edge_dims(2)))
+            vals, counts = np.unique(self.prec[lo_e:hi_e], return_counts=True)
+            nz = vals != 0.0
+            reg[lv.L] = vals[nz][np.argmax(counts[nz])] if nz.any() else 0.0
+            irregular[lo_e:hi_e] = self.prec[lo_e:hi_e] != reg[lv.L]
+        A["PREC_BITS"] = _bits(irregular)
+        A["PREC_REG"] = reg
+        self.prec_regular = reg
+        ie = np.nonzero(self.inlet)[0]
+        hz = np.where(lay.edge_axis[ie] == 2, lay.edge_h[ie], 0.0)
+        A["INLET_IDX"] = ie.astype(np.int32)
+        A["INLET_VAL"] = lay.epos[ie, 1] * hz
+        for name, M in (("CURL", ops.C), ("ROT", ops.R)):
+            A[name + "_PTR"], A[name + "_COL"], A[name + "_VAL"] = _csr_arrays(M)
+        f = np.nonzero(lay.face_exists)[0]
+        lo, hi = lay.face_lo[f], lay.face_hi[f]
+        mlo, mhi = lo >= 0, hi >= 0
+        vol_ci = ops.vol_ci
+        dlo = lay.fpos[f[mlo]] - lay.cpos[lo[mlo]]
+        dhi = lay.fpos[f[mhi]] - lay.cpos[hi[mhi]]
+        # interp_f2c: rows cells, cols faces, 3 values
+        rows = np.concatenate([lo[mlo], hi[mhi]])
+        cols = np.concatenate([f[mlo], f[mhi]])
+        v3 = np.concatenate([vol_ci[lo[mlo], None] * dlo, -vol_ci[hi[mhi], None] * dhi])
+        A["P_PTR"], A["P_COL"], A["P_VAL3"] = _triplets_sorted(rows, cols, v3, NC)
+        # integr_c2f: rows faces, cols cells
+        A["I_PTR"], A["I_COL"], A["I_VAL3"] = _triplets_sorted(cols, rows, np.concatenate([dlo, -dhi]), NF)
+        # cell -> signed faces (bit 0 set: the face's +a side is this cell)
+        code = np.concatenate([(f[mlo] << 1), (f[mhi] << 1) | 1]).astype(np.int64)
+        order = np.lexsort((code, rows))
+        ptr = np.zeros(NC + 1, dtype=np.int64)
+        np.add.at(ptr, rows + 1, 1)
+        A["CF_PTR"] = np.cumsum(ptr)
+        A["CF_FACE"] = code[order].astype(np.int32)
+        # face cells with ghost slots
+        bf = self.bfaces
+        gslot = np.full(NF, -1, dtype=np.int64)
+        gslot[bf] = NC + np.arange(bf.size)
+        flo = np.where(lay.face_lo >= 0, lay.face_lo, np.where(gslot >= 0, gslot, 0))
+        fhi = np.where(lay.face_hi >= 0, lay.face_hi, np.where(gslot >= 0, gslot, 0))
+        A["F_LO"] = flo.astype(np.int32)
+        A["F_HI"] = fhi.astype(np.int32)
+        A["F_AOL"] = ops.AoL
+        A["VOLCI"] = vol_ci
+        inner = np.where(lay.face_lo[bf] >= 0, lay.face_lo[bf], lay.face_hi[bf])
+        info = lay.face_axis[bf].astype(np.int32)
+        if self.cavity:
+            info |= 8
+        else:
+            info |= np.where(lay.face_bc[bf] == 1, 4, 0).astype(np.int32)
+        A["BF_FACE"] = bf.astype(np.int32)
+        A["BF_CELL"] = inner.astype(np.int32)
+        A["BF_INFO"] = info
+        A["BF_AF"] = lay.face_Af[bf]
+        # structured-matvec patches
+        plan = self.plan
+        for tag, (rows_p, M), n in (("PA", plan.patchA, NC), ("PV", plan.patchV, NC),
+                                    ("PR", plan.patchRI, NE)):
+            mask = np.zeros(n, dtype=bool)
+            mask[rows_p] = True
+            A[tag + "_BITS"] = _bits(mask)
+            A[tag + "_IDS"] = np.asarray(rows_p, dtype=np.int32)
+            A[tag + "_ROW"] = _rowmap(n, rows_p)
+            A[tag + "_PTR"], A[tag + "_COL"], A[tag + "_VAL"] = _csr_arrays(M)
+        self.patch_counts = (plan.patchA[0].size, plan.patchV[0].size, plan.patchRI[0].size)
+
+
+class DeviceSolver:
+    """One GPU context holding a nested layout, its operators and the solver state."""
+
+    def __init__(self, lay: NestedLayout, *, rou, visc, cavity, cg_check_interval=20,
+                 cg_max_iterations=1000, strict=False, ac=0.5, ad=0.5, tol1=1e-10, tol2=1e-9,
+                 device=0, precision="float64", mixed_tol=0.1, mixed_max_sweeps=200, tables=None):
+        if tables is None:
+            tables = LayoutTables(lay, cavity)
+        elif tables.lay is not lay or tables.cavity != bool(cavity):
+            raise ValueError("tables were built for another layout or boundary kind")
+        lay = tables.lay
+        self.lay = lay
+        self.tables = tables
+        self.ops = ops = tables.ops
+        self.cavity = tables.cavity
+        self.dir_mask = tables.dir_mask
+        self.inlet = tables.inlet
+        self.prec = tables.prec
+        self.plan = tables.plan
+        self.bfaces = tables.bfaces
+        self.prec_regular = tables.prec_regular
         NC, NF, NE = lay.NC, lay.NF, lay.NE
         L = _lib.Layout()
         L.nlevels = lay.N
@@ -100,89 +204,12 @@ class DeviceSolver:
 
     # ---- tables --------------------------------------------------------------
     def _upload_tables(self):
-        lay, ops, h = self.lay, self.ops, self.h
-        NC, NF, NE = lay.NC, lay.NF, lay.NE
-        h.upload("PREC", self.prec)
-        # per level, the value of the regular edges; edges that differ are flagged
-        reg = np.zeros(lay.N)
-        irregular = np.zeros(NE, dtype=bool)
-        for lv in lay.levels:
-            lo_e = lay.edge_base[lv.L][0]
-            hi_e = lay.edge_base[lv.L][2] + int(np.prod(lv.edge_dims(2)))
-            vals, counts = np.unique(self.prec[lo_e:hi_e], return_counts=True)
-            nz = vals != 0.0
-            reg[lv.L] = vals[nz][np.argmax(counts[nz])] if nz.any() else 0.0
-            irregular[lo_e:hi_e] = self.prec[lo_e:hi_e] != reg[lv.L]
-        h.upload("PREC_BITS", _bits(irregular))
-        h.upload("PREC_REG", reg)
-        self.prec_regular = reg
-        ie = np.nonzero(self.inlet)[0]
-        hz = np.where(lay.edge_axis[ie] == 2, lay.edge_h[ie], 0.0)
-        h.upload("INLET_IDX", ie.astype(np.int32))
-        h.upload("INLET_VAL", lay.epos[ie, 1] * hz)
-        for name, M in (("CURL", ops.C), ("ROT", ops.R)):
-            ptr, col, val = _csr_arrays(M)
-            h.upload(name + "_PTR", ptr)
-            h.upload(name + "_COL", col)
-            h.upload(name + "_VAL", val)
-        f = np.nonzero(lay.face_exists)[0]
-        lo, hi = lay.face_lo[f], lay.face_hi[f]
-        mlo, mhi = lo >= 0, hi >= 0
-        vol_ci = ops.vol_ci
-        dlo = lay.fpos[f[mlo]] - lay.cpos[lo[mlo]]
-        dhi = lay.fpos[f[mhi]] - lay.cpos[hi[mhi]]
-        # interp_f2c: rows cells, cols faces, 3 values
-        rows = np.concatenate([lo[mlo], hi[mhi]])
-        cols = np.concatenate([f[mlo], f[mhi]])
-        v3 = np.concatenate([vol_ci[lo[mlo], None] * dlo, -vol_ci[hi[mhi], None] * dhi])
-        ptr, col, val = _triplets_sorted(rows, cols, v3, NC)
-        h.upload("P_PTR", ptr); h.upload("P_COL", col); h.upload("P_VAL3", val)
-        # integr_c2f: rows faces, cols cells
-        ptr, col, val = _triplets_sorted(cols, rows, np.concatenate([dlo, -dhi]), NF)
-        h.upload("I_PTR", ptr); h.upload("I_COL", col); h.upload("I_VAL3", val)
-        # cell -> signed faces (bit 0 set: the face's +a side is this cell)
-        code = np.concatenate([(f[mlo] << 1), (f[mhi] << 1) | 1]).astype(np.int64)
-        order = np.lexsort((code, rows))
-        ptr = np.zeros(NC + 1, dtype=np.int64)
-        np.add.at(ptr, rows + 1, 1)
-        h.upload("CF_PTR", np.cumsum(ptr))
-        h.upload("CF_FACE", code[order].astype(np.int32))
-        # face cells with ghost slots
-        bf = self.bfaces
-        gslot = np.full(NF, -1, dtype=np.int64)
-        gslot[bf] = NC + np.arange(bf.size)
-        flo = np.where(lay.face_lo >= 0, lay.face_lo, np.where(gslot >= 0, gslot, 0))
-        fhi = np.where(lay.face_hi >= 0, lay.face_hi, np.where(gslot >= 0, gslot, 0))
-        h.upload("F_LO", flo.astype(np.int32))
-        h.upload("F_HI", fhi.astype(np.int32))
-        h.upload("F_AOL", ops.AoL)
-        h.upload("VOLCI", vol_ci)
-        inner = np.where(lay.face_lo[bf] >= 0, lay.face_lo[bf], lay.face_hi[bf])
-        info = lay.face_axis[bf].astype(np.int32)
-        if self.cavity:
-            info |= 8
-        else:
-            info |= np.where(lay.face_bc[bf] == 1, 4, 0).astype(np.int32)
-        h.upload("BF_FACE", bf.astype(np.int32))
-        h.upload("BF_CELL", inner.astype(np.int32))
-        h.upload("BF_INFO", info)
-        h.upload("BF_AF", lay.face_Af[bf])
-        # structured-matvec patches
-        plan = self.plan
-        for tag, (rows_p, M), n in (("PA", plan.patchA, NC), ("PV", plan.patchV, NC),
-                                    ("PR", plan.patchRI, NE)):
-            mask = np.zeros(n, dtype=bool)
-            mask[rows_p] = True
-            ptr, col, val = _csr_arrays(M)
-            h.upload(tag + "_BITS", _bits(mask))
-            h.upload(tag + "_IDS", np.asarray(rows_p, dtype=np.int32))
-            h.upload(tag + "_ROW", _rowmap(n, rows_p))
-            h.upload(tag + "_PTR", ptr)
-            h.upload(tag + "_COL", col)
-            h.upload(tag + "_VAL", val)
-        counts = (C.c_int64 * 3)(plan.patchA[0].size, plan.patchV[0].size, plan.patchRI[0].size)
+        h = self.h
+        for name, arr in self.tables.arrays.items():
+            h.upload(name, arr)
+        counts = (C.c_int64 * 3)(*self.tables.patch_counts)
         h.call("pyib_finalize", counts, 3)
-        h.upload("LC_CPOS", np.ascontiguousarray(lay.cpos))
+        h.upload("LC_CPOS", np.ascontiguousarray(self.lay.cpos))
 
     def _push_params(self):
         P = _lib.Params(**self.params)

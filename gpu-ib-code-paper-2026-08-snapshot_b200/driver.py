@@ -48,7 +48,7 @@ class B200Driver:
 
     def __init__(self, layout: NestedLayout, visc, rou=1.0, ac=0.5, ad=0.5, *,
                  cg_max_iterations=1000, fail_on_cg_nonconvergence=False, device=0,
-                 precision="float64", mixed_tol=0.1):
+                 precision="float64", mixed_tol=0.1, tables=None):
         if precision not in ("float64", "mixed"):
             raise ValueError("precision must be 'float64' or 'mixed'")
         self.precision = precision
@@ -79,6 +79,7 @@ class B200Driver:
         self.ib_implicit = False
         self.last_step_dt = None
         self.last_helm_m = 0
+        self._tables = tables          # shared LayoutTables of this layout (optional)
 
     # ---- configuration ------------------------------------------------------
     def set_cavity(self, U_lid=0.0, spanwise_zerograd=False):
@@ -118,7 +119,9 @@ class B200Driver:
                                         cg_max_iterations=self.cg_max_iterations,
                                         strict=self.fail_on_cg_nonconvergence, ac=self.ac, ad=self.ad,
                                         device=self.device, precision=self.precision,
-                                        mixed_tol=self.mixed_tol)
+                                        mixed_tol=self.mixed_tol,
+                                        tables=self._tables if self._tables is not None
+                                        and self._tables.cavity == self.cavity else None)
             self._ib_dirty = True
         sv = self._solver
         want = dict(check=int(self.cg_check_interval), cg_max=int(self.cg_max_iterations),

@@ -71,12 +71,15 @@ class SphereRun:
     """One sphere case on one GPU: driver, markers, loads and the current state."""
 
     def __init__(self, case: SphereCase, device=0, layout=None, check_interval=20,
-                 precision="float64", mixed_tol=0.1):
+                 precision="float64", mixed_tol=0.1, tables=None):
         self.case = case
-        lay = layout if layout is not None else case.layout()
+        if tables is not None:
+            lay = tables.lay
+        else:
+            lay = layout if layout is not None else case.layout()
         drv = B200Driver(lay, case.viscosity, case.density,
                          cg_max_iterations=case.cg_max_iterations, device=device,
-                         precision=precision, mixed_tol=mixed_tol)
+                         precision=precision, mixed_tol=mixed_tol, tables=tables)
         drv.cg_check_interval = int(check_interval)
         if case.cavity:
             drv.set_cavity(0.0, False)
