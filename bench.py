@@ -290,12 +290,15 @@ def run_b200(args, world, rank, local):
     from pyib_b200.cases import CASES
     from pyib_b200.runner import SphereRun
 
+    from pyib_b200.device import LayoutTables
+
     build.build_library()
     dist = maybe_init_dist(world, local)
     case = CASES[args.workload]
     t_setup = time.perf_counter()
+    tables = LayoutTables(case.layout().build(), case.cavity)
     run = SphereRun(case, device=local if world > 1 else 0, precision=args.precision,
-                    mixed_tol=args.mixed_tol)
+                    mixed_tol=args.mixed_tol, tables=tables)
     drv = run.drv
     sv = drv.solver
     setup_s = time.perf_counter() - t_setup
@@ -353,6 +356,13 @@ def run_b200(args, world, rank, local):
         traffic = d.get("bytes_per_edge_iteration", 0.0) * ne
     mv_achieved = ALGO_BYTES_PER_EDGE_MATVEC * ne / (mv_ms.value / 1e3) / 1e9
     M = drv.ib_markers.shape[0]
+    mixed = None
+    if world == 1 and args.precision == "float64" and not args.no_mixed:
+        final = dict(U=sv.get("U"), vc=np.asarray(run.vc).copy(), fL=np.asarray(drv.ib_force_L).copy(),
+                     force=np.asarray(run.loads.latest["body_force"]).copy())
+        steps_done = run.step_index
+        sv.h.close()
+        mixed = mixed_leg(case, tables, args, steps_done, final)
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -384,10 +394,42 @@ def run_b200(args, world, rank, local):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if mixed is not None:
+            mixed["speedup_vs_float64"] = mixed["value"] / value
+            line["mixed"] = mixed
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def mixed_leg(case, tables, args, steps_done, final):
+    """The mixed form on the same case and start: steps/s over ``args.steps`` steps
+    (CUDA events, after ``args.warmup`` steps) and, after the same total number of
+    steps as the float64 run, the relative errors of U, vc, fL and the body force."""
+    from pyib_b200.runner import SphereRun
+    run = SphereRun(case, device=0, precision="mixed", mixed_tol=args.mixed_tol, tables=tables)
+    sv = run.drv.solver
+    for _ in range(args.warmup):
+        run.advance()
+    ev = C.c_double(0.0)
+    its = 0
+    sv.h.call("pyib_event", 0, None)
+    for _ in range(args.steps):
+        run.advance()
+        its += run.drv.helmholtz_total_iterations_last_step
+    sv.h.call("pyib_event", 1, C.byref(ev))
+    while run.step_index < steps_done:
+        run.advance()
+    sv.h.call("pyib_calc_vel")
+    got = dict(U=sv.get("U"), vc=np.asarray(run.vc), fL=np.asarray(run.drv.ib_force_L),
+               force=np.asarray(run.loads.latest["body_force"]))
+    err = {k: float(np.linalg.norm(got[k] - final[k]) / max(np.linalg.norm(final[k]), 1e-300)) for k in got}
+    sv.h.close()
+    t = ev.value / 1000.0
+    return {"value": args.steps / t, "unit": "steps/s", "ms_per_step": 1000.0 * t / args.steps,
+            "inner_iterations_per_step": its / args.steps, "mixed_tolerance": args.mixed_tol,
+            "errors_vs_float64_after_steps": steps_done, "errors_vs_float64": err}
 
 
 # ---------------------------------------------------------------------------
@@ -508,11 +550,13 @@ def run_batch(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="d32_oscillating_sphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision leg of the default float64 run")
     ap.add_argument("--precision", default="float64", choices=["float64", "mixed"])
     ap.add_argument("--mixed-tol", type=float, default=0.1)
     ap.add_argument("--batch-cases", type=int, default=64)

@@ -57,9 +57,12 @@ struct Meta {
   long long nc, nf, ne;
   int kz;              // z planes marched by one cell tile (kernels A and V)
   int kzR;             // z planes marched by one node tile (kernel RI)
-  int gxA, gyA, gzA;   // cell-tile grid (kernels A and V)
+  int gxA, gyA, gzA;   // cell-tile grid (kernel A; kernel V uses gxV and the same y, z)
+  int gxV;             // x tiles of kernel V (two cells per thread: 64 cells a tile)
   int gxR, gyR, gzR;   // node-tile grid (kernel RI)
   int nplanes;         // per-plane partial sums of kernel RI (independent of the z-chunk depth)
+  int ri_up;           // 1: kernel RI also marches the upper-face nodes (i = nx, j = ny, k = nz);
+                       // 0: every upper-face edge is an exact (patch) row or masked
 };
 
 struct CGState {
@@ -284,24 +287,25 @@ __device__ __forceinline__ int level_of_zblock(const Meta& m, int bz, bool node_
 void set_grids(Meta& m, int kzA, int kzR) {
   m.kz = kzA;
   m.kzR = kzR;
-  int zA = 0, zR = 0, gxA = 1, gyA = 1, gxR = 1, gyR = 1;
+  int zA = 0, zR = 0, gxA = 1, gyA = 1, gxR = 1, gyR = 1, gxV = 1;
   for (int L = 0; L < m.nl; ++L) {
     LevelMeta& l = m.lv[L];
     l.zbA = zA;
     l.zbR = zR;
     zA += (l.n[2] + kzA - 1) / kzA;
-    zR += (l.n[2] + 1 + kzR - 1) / kzR;
+    zR += (l.n[2] + m.ri_up + kzR - 1) / kzR;
     gxA = std::max(gxA, (l.n[0] + TX - 1) / TX);
+    gxV = std::max(gxV, (l.n[0] + 2 * TX - 1) / (2 * TX));
     gyA = std::max(gyA, (l.n[1] + TY - 1) / TY);
-    gxR = std::max(gxR, (l.n[0] + 1 + TX - 1) / TX);
-    gyR = std::max(gyR, (l.n[1] + 1 + TY - 1) / TY);
+    gxR = std::max(gxR, (l.n[0] + m.ri_up + TX - 1) / TX);
+    gyR = std::max(gyR, (l.n[1] + m.ri_up + TY - 1) / TY);
   }
-  m.gxA = gxA; m.gyA = gyA; m.gzA = zA;
+  m.gxA = gxA; m.gyA = gyA; m.gzA = zA; m.gxV = gxV;
   m.gxR = gxR; m.gyR = gyR; m.gzR = zR;
   int pb = 0;
   for (int L = 0; L < m.nl; ++L) {
     m.lv[L].plane_base = pb;
-    pb += gxR * gyR * (m.lv[L].n[2] + 1);
+    pb += gxR * gyR * (m.lv[L].n[2] + m.ri_up);
   }
   m.nplanes = pb;
 }
@@ -364,67 +368,84 @@ __global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p
 
 // ---------------------------------------------------------------------------
 // matvec kernel V: vq = rou v - kfac * Vd v per component (7-point template with a
-// zero ghost at the domain boundary); the z-neighbours are carried in registers.
+// zero ghost at the domain boundary).  Each thread owns two x-consecutive cells
+// (a tile is 64 x 8 cells), so the pair shares its x-neighbour loads; the
+// z-neighbours are carried in registers.  Hole cells are skipped; rows of
+// irregular cells are overwritten by k_patchV.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v, T* __restrict__ vq,
-                                                  const unsigned int* __restrict__ pbits,
-                                                  const int* __restrict__ prow,
-                                                  const long long* __restrict__ pptr,
-                                                  const int* __restrict__ pcol,
-                                                  const T* __restrict__ pval,
                                                   const CGState* __restrict__ st) {
   if (st->done) return;
   const int L = level_of_zblock(m, blockIdx.z, false);
   const LevelMeta& l = m.lv[L];
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
-  const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
+  const int i = blockIdx.x * (2 * TX) + 2 * threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
   if (i >= nx || j >= ny) return;
+  const bool hasB = i + 1 < nx;                   // the second cell (i+1, j)
   const int k0 = (blockIdx.z - l.zbA) * m.kz;
   const int k1 = min(k0 + m.kz, nz);
   const long long nc = m.nc;
   const T rou = (T)st->rou, kf = (T)st->kfac;
   const T inv_h2 = (T)(1.0 / (l.h * l.h));
-  const long long cstep = (long long)nx * ny;
-  const long long c0 = l.cbase + ((long long)k0 * ny + j) * nx + i;
-  const bool col_hole = l.has_hole && i >= l.hole_lo[0] && i < l.hole_hi[0] && j >= l.hole_lo[1] &&
-                        j < l.hole_hi[1];
-  const bool xm = i > 0, xp = i + 1 < nx, ym = j > 0, yp = j + 1 < ny;
-  T vm[3], v0[3];
+  const int cs = nx * ny;
+  const bool row_hole = l.has_hole && j >= l.hole_lo[1] && j < l.hole_hi[1];
+  const bool holeA = row_hole && i >= l.hole_lo[0] && i < l.hole_hi[0];
+  const bool holeB = row_hole && i + 1 >= l.hole_lo[0] && i + 1 < l.hole_hi[0];
+  const bool xm = i > 0, xpB = i + 2 < nx, ym = j > 0, yp = j + 1 < ny;
+  const long long off = l.cbase + (long long)k0 * cs + (long long)j * nx + i;
+  const T* src = v + off;
+  T* dst = vq + off;
+  T am[3], a0[3], bm[3], b0[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    v0[d] = v[d * nc + c0];
-    vm[d] = k0 > 0 ? v[d * nc + c0 - cstep] : (T)0;
+    const T* sd = src + d * nc;
+    a0[d] = sd[0];
+    b0[d] = hasB ? sd[1] : (T)0;
+    am[d] = k0 > 0 ? sd[-cs] : (T)0;
+    bm[d] = (k0 > 0 && hasB) ? sd[1 - cs] : (T)0;
   }
-  long long c = c0;
-  for (int k = k0; k < k1; ++k, c += cstep) {
-    T vp[3];
+  for (int k = k0; k < k1; ++k) {
+    const bool zp = k + 1 < nz, zm = k > 0;
+    const bool zhole = k >= l.hole_lo[2] && k < l.hole_hi[2];
+    const bool doA = !(holeA && zhole), doB = hasB && !(holeB && zhole);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) vp[d] = k + 1 < nz ? v[d * nc + c + cstep] : (T)0;
-    if (!(col_hole && k >= l.hole_lo[2] && k < l.hole_hi[2])) {
-      // template for every cell; rows of irregular cells are overwritten by k_patchV
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const T* vd = v + d * nc;
-        const T vc0 = v0[d];
+    for (int d = 0; d < 3; ++d) {
+      const T* sd = src + d * nc;
+      const T ap = zp ? sd[cs] : (T)0;
+      const T bp = (zp && hasB) ? sd[cs + 1] : (T)0;
+      if (doA) {
+        const T x0 = a0[d];
         T acc = 0;
-        acc += xp ? vd[c + 1] - vc0 : -2 * vc0;
-        acc += xm ? vd[c - 1] - vc0 : -2 * vc0;
-        acc += yp ? vd[c + nx] - vc0 : -2 * vc0;
-        acc += ym ? vd[c - nx] - vc0 : -2 * vc0;
-        acc += (k + 1 < nz) ? vp[d] - vc0 : -2 * vc0;
-        acc += (k > 0) ? vm[d] - vc0 : -2 * vc0;
-        vq[d * nc + c] = rou * vc0 - kf * (acc * inv_h2);
+        acc += hasB ? b0[d] - x0 : -2 * x0;
+        acc += xm ? sd[-1] - x0 : -2 * x0;
+        acc += yp ? sd[nx] - x0 : -2 * x0;
+        acc += ym ? sd[-nx] - x0 : -2 * x0;
+        acc += zp ? ap - x0 : -2 * x0;
+        acc += zm ? am[d] - x0 : -2 * x0;
+        dst[d * nc] = rou * x0 - kf * (acc * inv_h2);
       }
+      if (doB) {
+        const T x0 = b0[d];
+        T acc = 0;
+        acc += xpB ? sd[2] - x0 : -2 * x0;
+        acc += a0[d] - x0;
+        acc += yp ? sd[nx + 1] - x0 : -2 * x0;
+        acc += ym ? sd[1 - nx] - x0 : -2 * x0;
+        acc += zp ? bp - x0 : -2 * x0;
+        acc += zm ? bm[d] - x0 : -2 * x0;
+        dst[d * nc + 1] = rou * x0 - kf * (acc * inv_h2);
+      }
+      am[d] = a0[d]; a0[d] = ap; bm[d] = b0[d]; b0[d] = bp;
     }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { vm[d] = v0[d]; v0[d] = vp[d]; }
+    src += cs;
+    dst += cs;
   }
 }
 
 // ---------------------------------------------------------------------------
-// matvec kernel RI: w = R I vq, fused with the dot p.w and alpha = eta / p.w.
-// Thread (i,j) of a 32x8 node tile marches kz node planes.  The face values
+// matvec kernel RI: w = R I vq, fused with the dot p.w (alpha = eta / p.w is set by
+// k_patchRI).  Thread (i,j) of a 32x8 node tile marches kz node planes.  The face values
 //   F_x(i,j,k) = (h/2)(vq_x(i-1,j,k) + vq_x(i,j,k)),  F_y likewise in y,
 //   F_z(i,j,k) = (h/2)(vq_z(i,j,k-1) + vq_z(i,j,k))
 // of the node and of its -x and -y neighbours come straight from (L1-cached)
@@ -432,16 +453,99 @@ __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v
 //   w_x(i,j,k) = F_z(i,j,k) - F_z(i,j-1,k) + F_y(i,j,k-1) - F_y(i,j,k)
 //   w_y(i,j,k) = F_x(i,j,k) - F_x(i,j,k-1) + F_z(i-1,j,k) - F_z(i,j,k)
 //   w_z(i,j,k) = F_y(i,j,k) - F_y(i-1,j,k) + F_x(i,j-1,k) - F_x(i,j,k)
+// The nodes on a level's upper faces (i = nx, j = ny, k = nz) carry only interface
+// and boundary edges.  When all of those are exact (patch) rows or masked -- every
+// closed-cavity layout -- the kernel marches only nodes i < nx, j < ny, k < nz
+// (ri_up = 0), so the node tiles are whole 32 x 8 tiles of the cell grid; otherwise
+// (ri_up = 1) it marches all nx+1 x ny+1 x nz+1 nodes.
 // ---------------------------------------------------------------------------
+template <typename T>
+struct RICarry {
+  T vz00, vzm0, vz0m;   // vq_z of cells (i,j), (i-1,j), (i,j-1) on the previous plane
+  T fy, fx;             // F_y(i,j), F_x(i,j) on the previous plane
+};
+
+// carried values of node (i,j) entering plane k0
+template <typename T>
+__device__ __forceinline__ void ri_start(const LevelMeta& l, int i, int j, int k0, const T* vx, const T* vy,
+                                         const T* vz, T hh, RICarry<T>& c) {
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const bool c00 = i < nx && j < ny, cm0 = i > 0 && i <= nx && j < ny, c0m = i < nx && j > 0 && j <= ny;
+  c.vz00 = c.vzm0 = c.vz0m = c.fy = c.fx = (T)0;
+  if (k0 > 0) {
+    const int ob = (k0 - 1) * (nx * ny) + j * nx + i;
+    c.vz00 = c00 ? vz[ob] : (T)0;
+    c.vzm0 = cm0 ? vz[ob - 1] : (T)0;
+    c.vz0m = c0m ? vz[ob - nx] : (T)0;
+    if (k0 - 1 < nz) {
+      if (i < nx) c.fy = hh * ((c0m ? vy[ob - nx] : (T)0) + (c00 ? vy[ob] : (T)0));
+      if (j < ny) c.fx = hh * ((cm0 ? vx[ob - 1] : (T)0) + (c00 ? vx[ob] : (T)0));
+    }
+  }
+}
+
+// the three edges of node (i,j) on plane k; returns their share of p.w (template edges)
+template <typename T>
+__device__ __forceinline__ double ri_plane(const LevelMeta& l, int i, int j, int k, const T* vx, const T* vy,
+                                           const T* vz, T hh, T* __restrict__ w, const T* __restrict__ p,
+                                           const unsigned int* __restrict__ pbits, int do_dot, RICarry<T>& c) {
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const bool c00 = i < nx && j < ny, cm0 = i > 0 && i <= nx && j < ny, c0m = i < nx && j > 0 && j <= ny,
+             cmm = i > 0 && j > 0 && i <= nx && j <= ny;
+  const bool zin = k < nz;
+  const int ob = k * (nx * ny) + j * nx + i;
+  const long long ex_e = l.ebase[0] + (long long)k * ((ny + 1) * nx) + j * nx + i;
+  const long long ey_e = l.ebase[1] + (long long)k * (ny * (nx + 1)) + j * (nx + 1) + i;
+  const long long ez_e = l.ebase[2] + (long long)k * ((ny + 1) * (nx + 1)) + j * (nx + 1) + i;
+  // loads that do not depend on the stencil: bitmask words and the dot's p values
+  const unsigned int bwx = (pbits && i < nx) ? pbits[ex_e >> 5] : 0u;
+  const unsigned int bwy = (pbits && j < ny) ? pbits[ey_e >> 5] : 0u;
+  const unsigned int bwz = (pbits && zin) ? pbits[ez_e >> 5] : 0u;
+  const T px = (do_dot && i < nx) ? p[ex_e] : (T)0;
+  const T py = (do_dot && j < ny) ? p[ey_e] : (T)0;
+  const T pz = (do_dot && zin) ? p[ez_e] : (T)0;
+  const T vz00 = (zin && c00) ? vz[ob] : (T)0;
+  const T vzm0 = (zin && cm0) ? vz[ob - 1] : (T)0;
+  const T vz0m = (zin && c0m) ? vz[ob - nx] : (T)0;
+  T fx = 0, fy = 0, fx_jm = 0, fy_im = 0;
+  if (zin) {
+    const T vx00 = c00 ? vx[ob] : (T)0, vxm0 = cm0 ? vx[ob - 1] : (T)0;
+    const T vy00 = c00 ? vy[ob] : (T)0, vy0m = c0m ? vy[ob - nx] : (T)0;
+    if (j < ny) fx = hh * (vxm0 + vx00);                                                     // F_x(i,j)
+    if (i < nx) fy = hh * (vy0m + vy00);                                                     // F_y(i,j)
+    if (j > 0) fx_jm = hh * ((cmm ? vx[ob - nx - 1] : (T)0) + (c0m ? vx[ob - nx] : (T)0));   // F_x(i,j-1)
+    if (i > 0) fy_im = hh * ((cmm ? vy[ob - nx - 1] : (T)0) + (cm0 ? vy[ob - 1] : (T)0));    // F_y(i-1,j)
+  }
+  const T fz = (i < nx && j < ny) ? hh * (c.vz00 + vz00) : (T)0;                             // F_z(i,j)
+  const T fz_im = (i > 0 && j < ny) ? hh * (c.vzm0 + vzm0) : (T)0;                           // F_z(i-1,j)
+  const T fz_jm = (i < nx && j > 0) ? hh * (c.vz0m + vz0m) : (T)0;                           // F_z(i,j-1)
+  // template for every edge; irregular edges are overwritten by k_patchRI, which also
+  // adds their share of the dot product
+  double dot = 0.0;
+  if (i < nx) {
+    const T val = fz - fz_jm + c.fy - fy;
+    w[ex_e] = val;
+    if (!((bwx >> (ex_e & 31)) & 1u)) dot += (double)px * (double)val;
+  }
+  if (j < ny) {
+    const T val = fx - c.fx + fz_im - fz;
+    w[ey_e] = val;
+    if (!((bwy >> (ey_e & 31)) & 1u)) dot += (double)py * (double)val;
+  }
+  if (zin) {
+    const T val = fy - fy_im + fx_jm - fx;
+    w[ez_e] = val;
+    if (!((bwz >> (ez_e & 31)) & 1u)) dot += (double)pz * (double)val;
+  }
+  c.vz00 = vz00; c.vzm0 = vzm0; c.vz0m = vz0m;
+  c.fx = fx; c.fy = fy;
+  return dot;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
                                                    const T* __restrict__ p,
-                                                   const unsigned int* __restrict__ pbits,
-                                                   const int* __restrict__ prow,
-                                                   const long long* __restrict__ pptr,
-                                                   const int* __restrict__ pcol,
-                                                   const T* __restrict__ pval, double* partials,
+                                                   const unsigned int* __restrict__ pbits, double* partials,
                                                    CGState* st, int do_dot) {
   if (st->done) return;
   static_assert(TY == 8, "the per-plane combine below assumes 8 warps per block");
@@ -451,86 +555,20 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
   const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
   const int k0 = (blockIdx.z - l.zbR) * m.kzR;
-  const int k1 = min(k0 + m.kzR, nz + 1);
+  const int k1 = min(k0 + m.kzR, nz + m.ri_up);
   const long long nc = m.nc;
   const T* vx = vq + l.cbase;
   const T* vy = vq + nc + l.cbase;
   const T* vz = vq + 2 * nc + l.cbase;
   const T hh = (T)(0.5 * l.h);
-  const int cs = nx * ny;
-  const bool act = i <= nx && j <= ny;
-  // cell-column validity (x,y) for the cells each face reads
-  const bool c00 = i < nx && j < ny;              // (i, j)
-  const bool cm0 = i > 0 && i <= nx && j < ny;    // (i-1, j)
-  const bool c0m = i < nx && j > 0 && j <= ny;    // (i, j-1)
-  const bool cmm = i > 0 && j > 0 && i <= nx && j <= ny;   // (i-1, j-1)
-  const int o00 = j * nx + i;
-  auto ld = [&](const T* a, bool ok, int o) -> T { return ok ? a[o] : (T)0; };
-  T vz00_m = 0, vzm0_m = 0, vz0m_m = 0;            // z-face inputs at plane k-1
-  T fy_m = 0, fx_m = 0;                            // F_y(i,j,k-1), F_x(i,j,k-1)
-  if (act && k0 > 0) {
-    const int ob = (k0 - 1) * cs + o00;
-    vz00_m = ld(vz, c00, ob);
-    vzm0_m = ld(vz, cm0, ob - 1);
-    vz0m_m = ld(vz, c0m, ob - nx);
-    if (k0 - 1 < nz) {
-      if (i < nx) fy_m = hh * (ld(vy, c0m, ob - nx) + ld(vy, c00, ob));
-      if (j < ny) fx_m = hh * (ld(vx, cm0, ob - 1) + ld(vx, c00, ob));
-    }
-  }
+  const bool act = i < nx + m.ri_up && j < ny + m.ri_up;
+  RICarry<T> c;
+  if (act) ri_start<T>(l, i, j, k0, vx, vy, vz, hh, c);
   for (int k = k0; k < k1; ++k) {
-    double dot[1] = {0.0};
-    if (act) {
-      const bool zin = k < nz;
-      const int ob = k * cs + o00;
-      const long long ex_e = l.ebase[0] + (long long)k * ((ny + 1) * nx) + j * nx + i;
-      const long long ey_e = l.ebase[1] + (long long)k * (ny * (nx + 1)) + j * (nx + 1) + i;
-      const long long ez_e = l.ebase[2] + (long long)k * ((ny + 1) * (nx + 1)) + j * (nx + 1) + i;
-      // loads that do not depend on the stencil: bitmask words and the dot's p values
-      const unsigned int bwx = (pbits && i < nx) ? pbits[ex_e >> 5] : 0u;
-      const unsigned int bwy = (pbits && j < ny) ? pbits[ey_e >> 5] : 0u;
-      const unsigned int bwz = (pbits && zin) ? pbits[ez_e >> 5] : 0u;
-      const T px = (do_dot && i < nx) ? p[ex_e] : (T)0;
-      const T py = (do_dot && j < ny) ? p[ey_e] : (T)0;
-      const T pz = (do_dot && zin) ? p[ez_e] : (T)0;
-      const T vz00 = zin ? ld(vz, c00, ob) : (T)0;
-      const T vzm0 = zin ? ld(vz, cm0, ob - 1) : (T)0;
-      const T vz0m = zin ? ld(vz, c0m, ob - nx) : (T)0;
-      T fx = 0, fy = 0, fx_jm = 0, fy_im = 0;
-      if (zin) {
-        const T vx00 = ld(vx, c00, ob), vxm0 = ld(vx, cm0, ob - 1);
-        const T vy00 = ld(vy, c00, ob), vy0m = ld(vy, c0m, ob - nx);
-        if (j < ny) fx = hh * (vxm0 + vx00);                                          // F_x(i,j)
-        if (i < nx) fy = hh * (vy0m + vy00);                                          // F_y(i,j)
-        if (j > 0) fx_jm = hh * (ld(vx, cmm, ob - nx - 1) + ld(vx, c0m, ob - nx));    // F_x(i,j-1)
-        if (i > 0) fy_im = hh * (ld(vy, cmm, ob - nx - 1) + ld(vy, cm0, ob - 1));     // F_y(i-1,j)
-      }
-      const T fz = (i < nx && j < ny) ? hh * (vz00_m + vz00) : (T)0;                 // F_z(i,j)
-      const T fz_im = (i > 0 && j < ny) ? hh * (vzm0_m + vzm0) : (T)0;               // F_z(i-1,j)
-      const T fz_jm = (i < nx && j > 0) ? hh * (vz0m_m + vz0m) : (T)0;               // F_z(i,j-1)
-      // template for every edge; irregular edges are overwritten by k_patchRI, which
-      // also adds their share of the dot product
-      if (i < nx) {
-        const T val = fz - fz_jm + fy_m - fy;
-        w[ex_e] = val;
-        if (!((bwx >> (ex_e & 31)) & 1u)) dot[0] += (double)px * (double)val;
-      }
-      if (j < ny) {
-        const T val = fx - fx_m + fz_im - fz;
-        w[ey_e] = val;
-        if (!((bwy >> (ey_e & 31)) & 1u)) dot[0] += (double)py * (double)val;
-      }
-      if (zin) {
-        const T val = fy - fy_im + fx_jm - fx;
-        w[ez_e] = val;
-        if (!((bwz >> (ez_e & 31)) & 1u)) dot[0] += (double)pz * (double)val;
-      }
-      vz00_m = vz00; vzm0_m = vzm0; vz0m_m = vz0m;
-      fx_m = fx; fy_m = fy;
-    }
+    const double dot = act ? ri_plane<T>(l, i, j, k, vx, vy, vz, hh, w, p, pbits, do_dot, c) : 0.0;
     if (do_dot) {
       // warp sum of this plane, kept per (plane, warp) until the end of the block
-      double t = dot[0];
+      double t = dot;
       for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
       if (threadIdx.x == 0) swarp[k - k0][threadIdx.y] = t;
     }
@@ -1424,7 +1462,7 @@ int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* 
                     int do_dot, const T* pa_val, const T* pv_val, const T* pr_val) {
   const Meta& m = ctx->meta;
   const long long nc = ctx->lay.ncell;
-  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
+  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
   k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, pa_val, ctx->nA,
                                         ctx->st);
   CKL();
@@ -1436,7 +1474,7 @@ int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* 
   }
   const T* vsrc = vcm;
   if (alpd) {
-    k_mvV<T><<<gA, blk, 0, ctx->stream>>>(m, vcm, vq, nullptr, nullptr, nullptr, nullptr, pv_val, ctx->st);
+    k_mvV<T><<<gV, blk, 0, ctx->stream>>>(m, vcm, vq, ctx->st);
     CKL();
     if (ctx->nV > 0) {
       k_patchV<T><<<patch_grid(3 * ctx->nV), kThreads, 0, ctx->stream>>>(
@@ -1446,9 +1484,8 @@ int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* 
     }
     vsrc = vq;
   }
-  k_mvRI<T><<<gR, blk, 0, ctx->stream>>>(
-      m, vsrc, out, pdot, tp<unsigned int>(ctx, PYIB_T_PR_BITS), nullptr, nullptr, nullptr, pr_val,
-      ctx->partials, ctx->st, do_dot);
+  k_mvRI<T><<<gR, blk, 0, ctx->stream>>>(m, vsrc, out, pdot, tp<unsigned int>(ctx, PYIB_T_PR_BITS),
+                                          ctx->partials, ctx->st, do_dot);
   CKL();
   k_patchRI<T><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
       ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL),
@@ -2022,6 +2059,7 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
   // meta
   Meta& m = ctx->meta;
   m.nl = layout->nlevels;
+  m.ri_up = 1;                     // until pyib_finalize knows the upper faces are exact
   long long cb = 0, fb = 0, eb = 0;
   for (int L = 0; L < m.nl; ++L) {
     LevelMeta& l = m.lv[L];
@@ -2179,6 +2217,8 @@ int pyib_finalize(pyib_ctx* ctx, const int64_t* counts, int32_t ncounts) {
   ctx->nA = counts[0];
   ctx->nV = counts[1];
   ctx->nR = counts[2];
+  ctx->meta.ri_up = (ncounts >= 4 && counts[3] != 0) ? 0 : 1;
+  set_grids(ctx->meta, ctx->meta.kz, ctx->meta.kzR);
   if ((long long)ctx->meta.gxR * ctx->meta.gyR * ctx->meta.gzR + patch_grid(ctx->nR) > kPartStride ||
       (long long)ctx->meta.nplanes + patch_grid(ctx->nR) > kPartStride)
     return set_err(ctx, PYIB_E_ARG, "too many reduction slots for this layout");
@@ -2460,7 +2500,7 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
   // intermediate it reads is current)
   const Meta& m = ctx->meta;
   const long long nc = ctx->lay.ncell;
-  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
+  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
   for (int kern = 0; kern < 6; ++kern) {
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int q = 0; q < reps; ++q) {
@@ -2471,16 +2511,14 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
                     ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR),
                     tp<int>(ctx, PYIB_T_PA_COL), tp<double>(ctx, PYIB_T_PA_VAL), ctx->work_e, ctx->vcm, nc,
                     ctx->st); break;
-        case 2: k_mvV<double><<<gA, blk, 0, ctx->stream>>>(m, ctx->vcm, ctx->vq, nullptr, nullptr, nullptr,
-                                                           nullptr, nullptr, ctx->st); break;
+        case 2: k_mvV<double><<<gV, blk, 0, ctx->stream>>>(m, ctx->vcm, ctx->vq, ctx->st); break;
         case 3: k_patchV<double><<<patch_grid(3 * ctx->nV), kThreads, 0, ctx->stream>>>(
                     ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR),
                     tp<int>(ctx, PYIB_T_PV_COL), tp<double>(ctx, PYIB_T_PV_VAL), ctx->vcm, ctx->vq, nc,
                     ctx->st); break;
         case 4: k_mvRI<double><<<gR, blk, 0, ctx->stream>>>(m, ctx->vq, ctx->work_e2, ctx->work_e,
-                                                            tp<unsigned int>(ctx, PYIB_T_PR_BITS), nullptr,
-                                                            nullptr, nullptr, nullptr, ctx->partials, ctx->st,
-                                                            1); break;
+                                                            tp<unsigned int>(ctx, PYIB_T_PR_BITS), ctx->partials,
+                                                            ctx->st, 1); break;
         default: k_patchRI<double><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
                     ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR),
                     tp<int>(ctx, PYIB_T_PR_COL), tp<double>(ctx, PYIB_T_PR_VAL), ctx->vq, ctx->work_e2,

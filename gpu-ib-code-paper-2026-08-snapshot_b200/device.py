@@ -149,7 +149,8 @@ class LayoutTables:
             A[tag + "_IDS"] = np.asarray(rows_p, dtype=np.int32)
             A[tag + "_ROW"] = _rowmap(n, rows_p)
             A[tag + "_PTR"], A[tag + "_COL"], A[tag + "_VAL"] = _csr_arrays(M)
-        self.patch_counts = (plan.patchA[0].size, plan.patchV[0].size, plan.patchRI[0].size)
+        self.patch_counts = (plan.patchA[0].size, plan.patchV[0].size, plan.patchRI[0].size,
+                             int(plan.upper_exact))
 
 
 class DeviceSolver:
@@ -207,8 +208,8 @@ class DeviceSolver:
         h = self.h
         for name, arr in self.tables.arrays.items():
             h.upload(name, arr)
-        counts = (C.c_int64 * 3)(*self.tables.patch_counts)
-        h.call("pyib_finalize", counts, 3)
+        counts = (C.c_int64 * 4)(*self.tables.patch_counts)
+        h.call("pyib_finalize", counts, 4)
         h.upload("LC_CPOS", np.ascontiguousarray(self.lay.cpos))
 
     def _push_params(self):

@@ -26,6 +26,8 @@ from __future__ import annotations
 import numpy as np
 import scipy.sparse as sp
 
+from .layout import _grid
+
 
 def edge_views(lay, vec):
     """Per level, the three edge arrays of a dense edge vector as (z,y,x) views."""
@@ -181,6 +183,10 @@ class MatvecPlan:
             vq = rng.standard_normal((3, lay.NC))
             exw = ops.R @ sum(ops.I[d] @ vq[d] for d in range(3))
             irrRI |= _differs(t_RI(lay, vq), exw) & self.mask
+        # the edges of the nodes on a level's upper faces (i = nx, j = ny or k = nz) are
+        # interface or boundary edges; when every one of them is already an exact row or
+        # masked (closed cavities), the RI kernel covers only nodes i < nx, j < ny, k < nz
+        self.upper_exact = not np.any(upper_face_edges(lay) & self.mask & ~irrRI)
         self.irrA, self.irrV, self.irrRI = irrA, irrV, irrRI
         ra = np.nonzero(irrA)[0]
         # exact composite rows: component-major blocks of the same cell list
@@ -217,6 +223,17 @@ class MatvecPlan:
         return dict(patchA=int(self.patchA[0].size), patchV=int(self.patchV[0].size),
                     patchRI=int(self.patchRI[0].size), nnzA=int(self.patchA[1].nnz),
                     nnzV=int(self.patchV[1].nnz), nnzRI=int(self.patchRI[1].nnz))
+
+
+def upper_face_edges(lay):
+    """Edges whose lower node lies on an upper face of its level box (a coordinate == n)."""
+    out = np.zeros(lay.NE, dtype=bool)
+    for lv in lay.levels:
+        for a in range(3):
+            g = _grid(lv.edge_dims(a))
+            up = np.any(g == lv.n, axis=1)
+            out[lay.edge_id(lv.L, a, g[up])] = True
+    return out
 
 
 def _differs(a, b, rtol=1e-12):

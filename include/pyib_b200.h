@@ -155,7 +155,9 @@ int pyib_version(char* buf, size_t n);
 /* Host tables (IBCore.__init__ device transfer, ib_core_np.py:123-126;
  * build_A upload, ib_sparse.py:93-95).  bytes must match the table's type. */
 int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes);
-/* Patch-table row counts and matvec template constants; call after uploads. */
+/* Patch-table row counts {A rows, V rows, RI rows[, upper faces exact]}; call after
+ * uploads.  A fourth count != 0 states that every edge of the nodes on a level's
+ * upper faces is an RI patch row or masked, so the RI template skips those nodes. */
 int pyib_finalize(pyib_ctx* ctx, const int64_t* counts, int32_t ncounts);
 int pyib_set_params(pyib_ctx* ctx, const pyib_params* params);
 /* Marker-stencil geometry (ImmersedBoundary.__init__, ib_immersed.py:25-44). */
