@@ -425,11 +425,17 @@ def mixed_leg(case, tables, args, steps_done, final):
     got = dict(U=sv.get("U"), vc=np.asarray(run.vc), fL=np.asarray(run.drv.ib_force_L),
                force=np.asarray(run.loads.latest["body_force"]))
     err = {k: float(np.linalg.norm(got[k] - final[k]) / max(np.linalg.norm(final[k]), 1e-300)) for k in got}
+    mv = (C.c_double * 7)()
+    sv.set("WORK_E", np.random.default_rng(0).standard_normal(sv.lay.NE) * sv.lay.edge_exists)
+    sv.h.call("pyib_bench_matvec", 50, C.c_double(run.dt), mv)
+    kernels = dict(zip(["matvec", "curl_interp", "curl_interp_patch", "viscous", "viscous_patch",
+                        "integr_rot_dot", "integr_rot_patch_reduce"], [float(x) for x in mv]))
     sv.h.close()
     t = ev.value / 1000.0
     return {"value": args.steps / t, "unit": "steps/s", "ms_per_step": 1000.0 * t / args.steps,
             "inner_iterations_per_step": its / args.steps, "mixed_tolerance": args.mixed_tol,
-            "errors_vs_float64_after_steps": steps_done, "errors_vs_float64": err}
+            "errors_vs_float64_after_steps": steps_done, "errors_vs_float64": err,
+            "float32_matvec_kernel_ms": kernels}
 
 
 # ---------------------------------------------------------------------------
@@ -487,6 +493,56 @@ def run_precision_compare(args, world, rank, local):
         "mixed": {"steps_per_s": args.steps / mix["seconds"], "inner_iterations": mix["iterations"]},
         "errors_vs_float64": {k: rel(mix[k], f64[k]) for k in ("s", "U", "vc", "fL", "fE", "force")},
     }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Force harmonic error of the full oscillation run, float64 and mixed
+# ---------------------------------------------------------------------------
+def run_harmonic(args, world, rank, local):
+    """Six periods of the workload in float64 and in mixed precision; the axial body
+    force of each is fitted over 4T < t <= 6T against the analytic unsteady-Stokes
+    force (``pyib_b200.harmonic``), and the two harmonic errors are compared."""
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    from pyib_b200 import build
+    from pyib_b200.cases import CASES, R
+    from pyib_b200.device import LayoutTables
+    from pyib_b200.harmonic import harmonic_error
+    from pyib_b200.runner import SphereRun
+
+    build.build_library()
+    if world > 1:
+        raise SystemExit("the harmonic run uses one GPU")
+    case = CASES[args.workload]
+    if case.amplitude == 0.0:
+        raise SystemExit("the harmonic check needs an oscillating case")
+    tables = LayoutTables(case.layout().build(), case.cavity)
+    steps = args.periods * case.steps_per_period
+    axis = np.asarray(case.axis, dtype=np.float64) / np.linalg.norm(case.axis)
+    mu = case.viscosity
+    out = {}
+    for prec in ("float64", "mixed"):
+        run = SphereRun(case, device=0, tables=tables, precision=prec, mixed_tol=args.mixed_tol)
+        sv = run.drv.solver
+        times, fax, its = [], [], 0
+        ev = C.c_double(0.0)
+        sv.h.call("pyib_event", 0, None)
+        for _ in range(steps):
+            load = run.advance()
+            times.append(run.step_index * run.dt)
+            fax.append(float(np.asarray(load["body_force"]) @ axis))
+            its += run.drv.helmholtz_total_iterations_last_step
+        sv.h.call("pyib_event", 1, C.byref(ev))
+        sv.h.close()
+        err = harmonic_error(times, fax, mu=mu, radius=R, amplitude=case.amplitude, omega=case.omega,
+                             phase=case.phase, nu=mu / case.density)
+        out[prec] = {"steps_per_s": steps / (ev.value / 1000.0), "cg_iterations": its, **err}
+    diff_pp = 100.0 * abs(out["mixed"]["harmonic_vector_error"] - out["float64"]["harmonic_vector_error"])
+    line = {"metric": "force harmonic error, float64 and mixed", "workload": case.name, "steps": steps,
+            "periods": args.periods, "mixed_tolerance": args.mixed_tol, "float64": out["float64"],
+            "mixed": out["mixed"], "difference_percentage_points": diff_pp}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -560,6 +616,9 @@ def main():
     ap.add_argument("--precision", default="float64", choices=["float64", "mixed"])
     ap.add_argument("--mixed-tol", type=float, default=0.1)
     ap.add_argument("--batch-cases", type=int, default=64)
+    ap.add_argument("--harmonic", action="store_true",
+                    help="run --periods oscillation periods in float64 and mixed and fit the force")
+    ap.add_argument("--periods", type=int, default=6)
     ap.add_argument("--compare-precision", action="store_true",
                     help="run the workload in float64 and mixed precision and report the errors")
     args = ap.parse_args()
@@ -574,6 +633,8 @@ def main():
         return run_batch(args, world, rank, local)
     if args.compare_precision:
         return run_precision_compare(args, world, rank, local)
+    if args.harmonic:
+        return run_harmonic(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     return run_b200(args, world, rank, local)

@@ -614,7 +614,8 @@ __global__ void __launch_bounds__(kThreads) k_patchA(long long nA, const int* __
   vc[(q / nA) * nc + ids[q % nA]] = csr_row<T>(ptr, col, val, p, q);
 }
 
-// vq rows: the same Vd row for the three components of cell ids[r]
+// vq rows: the same Vd row for the three components of cell ids[r], one thread per row
+// (the row's columns and values are loaded once for the three gathers)
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __restrict__ ids,
                                                      const long long* __restrict__ ptr,
@@ -622,12 +623,22 @@ __global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __
                                                      const T* __restrict__ v, T* vq, long long nc,
                                                      const CGState* __restrict__ st) {
   if (st->done) return;
-  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (q >= 3 * nV) return;
-  const long long d = q / nV, r = q % nV;
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= nV) return;
   const int c = ids[r];
-  const T* vd = v + d * nc;
-  vq[d * nc + c] = (T)st->rou * vd[c] - (T)st->kfac * csr_row<T>(ptr, col, val, vd, r);
+  const long long q0 = ptr[r], q1 = ptr[r + 1];
+  T a0 = 0, a1 = 0, a2 = 0;
+  for (long long q = q0; q < q1; ++q) {
+    const T vv = val[q];
+    const int cc = col[q];
+    a0 += vv * v[cc];
+    a1 += vv * v[nc + cc];
+    a2 += vv * v[2 * nc + cc];
+  }
+  const T rou = (T)st->rou, kf = (T)st->kfac;
+  vq[c] = rou * v[c] - kf * a0;
+  vq[nc + c] = rou * v[nc + c] - kf * a1;
+  vq[2 * nc + c] = rou * v[2 * nc + c] - kf * a2;
 }
 
 // w rows (columns index the component-major vq), plus their share of p.w; the
@@ -1477,7 +1488,7 @@ int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* 
     k_mvV<T><<<gV, blk, 0, ctx->stream>>>(m, vcm, vq, ctx->st);
     CKL();
     if (ctx->nV > 0) {
-      k_patchV<T><<<patch_grid(3 * ctx->nV), kThreads, 0, ctx->stream>>>(
+      k_patchV<T><<<patch_grid(ctx->nV), kThreads, 0, ctx->stream>>>(
           ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL),
           pv_val, vcm, vq, nc, ctx->st);
       CKL();
@@ -2035,6 +2046,52 @@ int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* ma
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// Times reps back-to-back matvecs in -> out, then each of its kernels alone (benchmark
+// support for pyib_bench_matvec).
+template <typename T>
+int bench_matvec_t(pyib_ctx* ctx, int reps, const T* in, T* out, T* vcm, T* vq, const T* pa, const T* pv,
+                   const T* pr, double* ms_per) {
+  RET(launch_matvec_t<T>(ctx, in, out, vcm, vq, in, 1, 0, pa, pv, pr));   // warm
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  for (int q = 0; q < reps; ++q) RET(launch_matvec_t<T>(ctx, in, out, vcm, vq, in, 1, 0, pa, pv, pr));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ms_per[0] = ms / reps;
+  // each kernel alone, same inputs (after a full matvec, so every intermediate is current)
+  const Meta& m = ctx->meta;
+  const long long nc = ctx->lay.ncell;
+  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
+  for (int kern = 0; kern < 6; ++kern) {
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int q = 0; q < reps; ++q) {
+      switch (kern) {
+        case 0: k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                      ctx->nA, ctx->st); break;
+        case 1: k_patchA<T><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
+                    ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR),
+                    tp<int>(ctx, PYIB_T_PA_COL), pa, in, vcm, nc, ctx->st); break;
+        case 2: k_mvV<T><<<gV, blk, 0, ctx->stream>>>(m, vcm, vq, ctx->st); break;
+        case 3: k_patchV<T><<<patch_grid(ctx->nV), kThreads, 0, ctx->stream>>>(
+                    ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR),
+                    tp<int>(ctx, PYIB_T_PV_COL), pv, vcm, vq, nc, ctx->st); break;
+        case 4: k_mvRI<T><<<gR, blk, 0, ctx->stream>>>(m, vq, out, in, tp<unsigned int>(ctx, PYIB_T_PR_BITS),
+                                                       ctx->partials, ctx->st, 1); break;
+        default: k_patchRI<T><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
+                    ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR),
+                    tp<int>(ctx, PYIB_T_PR_COL), pr, vq, out, in, ctx->partials, m.nplanes, ctx->st, 1); break;
+      }
+      CKL();
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ms_per[1 + kern] = ms / reps;
+  }
+  return PYIB_OK;
+}
+
 extern "C" {
 
 int pyib_version(char* buf, size_t n) {
@@ -2488,50 +2545,18 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
   CK(cudaSetDevice(ctx->device));
   RET(tune_matvec(ctx));
   RET(set_state_solver(ctx, dt, 1));
-  RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));   // warm
-  CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  for (int q = 0; q < reps; ++q) RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  CK(cudaEventSynchronize(ctx->ev1));
-  float ms = 0.f;
-  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  ms_per[0] = ms / reps;
-  // each kernel of the matvec alone, same inputs (run after a full matvec, so every
-  // intermediate it reads is current)
-  const Meta& m = ctx->meta;
-  const long long nc = ctx->lay.ncell;
-  const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
-  for (int kern = 0; kern < 6; ++kern) {
-    CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (int q = 0; q < reps; ++q) {
-      switch (kern) {
-        case 0: k_mvA<double><<<gA, blk, 0, ctx->stream>>>(m, ctx->work_e, ctx->vcm, nullptr, nullptr, nullptr,
-                                                           nullptr, nullptr, ctx->nA, ctx->st); break;
-        case 1: k_patchA<double><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
-                    ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR),
-                    tp<int>(ctx, PYIB_T_PA_COL), tp<double>(ctx, PYIB_T_PA_VAL), ctx->work_e, ctx->vcm, nc,
-                    ctx->st); break;
-        case 2: k_mvV<double><<<gV, blk, 0, ctx->stream>>>(m, ctx->vcm, ctx->vq, ctx->st); break;
-        case 3: k_patchV<double><<<patch_grid(3 * ctx->nV), kThreads, 0, ctx->stream>>>(
-                    ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR),
-                    tp<int>(ctx, PYIB_T_PV_COL), tp<double>(ctx, PYIB_T_PV_VAL), ctx->vcm, ctx->vq, nc,
-                    ctx->st); break;
-        case 4: k_mvRI<double><<<gR, blk, 0, ctx->stream>>>(m, ctx->vq, ctx->work_e2, ctx->work_e,
-                                                            tp<unsigned int>(ctx, PYIB_T_PR_BITS), ctx->partials,
-                                                            ctx->st, 1); break;
-        default: k_patchRI<double><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
-                    ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR),
-                    tp<int>(ctx, PYIB_T_PR_COL), tp<double>(ctx, PYIB_T_PR_VAL), ctx->vq, ctx->work_e2,
-                    ctx->work_e, ctx->partials, m.nplanes, ctx->st, 1); break;
-      }
-      CKL();
-    }
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    CK(cudaEventSynchronize(ctx->ev1));
-    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    ms_per[1 + kern] = ms / reps;
+  if (ctx->prm.precision == 1) {
+    // the float32 matvec of the mixed solver, on a float32 copy of WORK_E
+    RET(ensure_mixed(ctx));
+    const long long ne = ctx->lay.nedge;
+    k_d2f<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->work_e, ctx->p32);
+    CKL();
+    return bench_matvec_t<float>(ctx, reps, ctx->p32, ctx->w32, ctx->vcm32, ctx->vq32, ctx->pa_val32,
+                                 ctx->pv_val32, ctx->pr_val32, ms_per);
   }
-  return PYIB_OK;
+  return bench_matvec_t<double>(ctx, reps, ctx->work_e, ctx->work_e2, ctx->vcm, ctx->vq,
+                                tp<double>(ctx, PYIB_T_PA_VAL), tp<double>(ctx, PYIB_T_PV_VAL),
+                                tp<double>(ctx, PYIB_T_PR_VAL), ms_per);
 }
 
 }  // extern "C"

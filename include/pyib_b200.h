@@ -224,7 +224,8 @@ int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms);
  * events (benchmark support).  ms_per holds 7 doubles: [0] one matvec, then one
  * launch of each of its kernels alone: [1] curl+interp template, [2] its patch
  * rows, [3] viscous template, [4] its patch rows, [5] integr+rot template with the
- * dot, [6] its patch rows with the final reduction. */
+ * dot, [6] its patch rows with the final reduction.  With params.precision = 1 the
+ * float32 matvec of the mixed solver is timed instead (on a float32 copy of WORK_E). */
 int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
 
 /* Deterministic spreading that allocates nothing.  No counterpart in the reference.
