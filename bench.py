@@ -167,7 +167,7 @@ def reference_sample(case, iters_per_step, cg_iters=6, threads=None):
     The sample runs the oracle's stencils (calc_vel, conv_diff, rot(integr_c2f))
     and ``cg_iters`` PCG iterations (matrix-free flow_mat + vector updates, the
     reference's CPU algorithm) on the same three-level oscillating-sphere
-    layout at D = 8 cells (92,160 cells; the full D = 32 layout needs several
+    layout at D = 8 cells (90,112 cells; the full D = 32 layout needs several
     minutes and ~20 GB just to assemble the oracle's geometry).  Costs are
     scaled to the full layout by edge count (per-edge work is the same) and
     to one step by the CG iteration count per step of the full case.
@@ -254,6 +254,8 @@ def full_cell_count(case):
 
 
 def run_reference(args, world, rank):
+    import _pyib_b200_import
+    _pyib_b200_import.load()
     from pyib_b200.cases import CASES
     case = CASES[args.workload]
     if rank != 0:
