@@ -374,7 +374,7 @@ def run_b200(args, world, rank, local):
             "metric": "D32 sphere steps/s", "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
+            "data": "synthetic", "cell_updates_per_s": value * int(sv.lay.cell_active.sum()),
             "config": {"workload": case.name, "cells": int(sv.lay.cell_active.sum()), "edges": ne,
                        "levels": sv.lay.N, "markers": M, "precision": args.precision,
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (working set > 2 GB)",
