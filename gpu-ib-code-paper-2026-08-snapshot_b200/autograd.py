@@ -1,0 +1,120 @@
+"""``torch.autograd.Function`` wrappers of the step's linear pieces and their adjoints.
+
+These are building blocks of a discrete adjoint of the step, run by the same
+hand-written kernels as the forward path:
+
+* ``HelmholtzSolve``: the stream-function solve of ``Driver.helm_solve``
+  (``ib_driver_np.py:311-410``), ``x = s + A_ff^-1 res_f`` on the free edges
+  (``x = s`` on masked edges).  A is symmetric, so the adjoint is the same PCG
+  on the masked incoming gradient from a zero start; the gradient with respect
+  to ``s`` is the identity.
+* ``MarkerInterp``: ``u_L = sum_k w_k vc[cell_k] hh^3`` (``ib_immersed.py:87-93``).
+  Its transpose is spreading with ``hh^3`` in place of the marker volumes.
+* ``MarkerSpread``: ``f_E = sum w f_L ds^3`` (``ib_immersed.py:103-111``).  Its
+  transpose is interpolation scaled by ``ds^3 / hh^3`` per marker.
+
+The stencil (cells and weights) is the one of the markers last set on the
+solver; derivatives with respect to marker positions (through the weights)
+are not part of these blocks.  Tensors are float64 in the solver's dense
+layout (edges: ``NE``; cell vectors: ``(3, NC)``; markers: ``(M, 3)``) on any
+device: they cross the C ABI as host arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def _np(t):
+    return t.detach().to("cpu", torch.float64).contiguous().numpy()
+
+
+def _like(a, ref):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(ref.device)
+
+
+def solve(solver, res_e, s, dt):
+    """One Helmholtz solve on the device: returns x (float64, dense edges)."""
+    solver.set("RES_E", res_e)
+    solver.set("S", s)
+    st = _lib.SolveStats()
+    solver.h.call("pyib_helm_solve", C.c_double(dt), C.byref(st))
+    return solver.get("S")
+
+
+class HelmholtzSolve(torch.autograd.Function):
+    """x = helm_solve(res_e, s); backward solves A y = mask * grad_x."""
+
+    @staticmethod
+    def forward(ctx, res_e, s, solver, dt):
+        ctx.solver, ctx.dt = solver, float(dt)
+        return _like(solve(solver, _np(res_e), _np(s), ctx.dt), res_e)
+
+    @staticmethod
+    def backward(ctx, grad_x):
+        sv = ctx.solver
+        free = sv.prec != 0.0
+        g = _np(grad_x) * free
+        y = solve(sv, g, np.zeros_like(g), ctx.dt) * free
+        return _like(y, grad_x), grad_x, None, None
+
+
+def _stencil(solver):
+    solver.h.call("pyib_ib_stencil")
+
+
+def interp(solver, vc3):
+    """u_L (M, 3) from a cell vector field (3, NC)."""
+    lay = solver.lay
+    full = np.zeros((3, lay.NC + solver.bfaces.size))
+    full[:, :lay.NC] = vc3
+    solver.set("VC", full)
+    _stencil(solver)
+    solver.h.call("pyib_ib_interp")
+    return solver.get("LAG_TMP").reshape(-1, 3)
+
+
+def spread(solver, f_l, ds):
+    """f_E (3, NC) = sum w f_L ds^3, with the given per-marker widths ``ds``."""
+    solver.set("DS", np.asarray(ds, dtype=np.float64) ** 3)
+    solver.set("FL", f_l)
+    _stencil(solver)
+    solver.h.call("pyib_ib_spread")
+    return solver.get("FE").reshape(3, -1)
+
+
+class MarkerInterp(torch.autograd.Function):
+    """u_L = interp(vc); backward spreads grad_u with hh^3 weights."""
+
+    @staticmethod
+    def forward(ctx, vc3, solver, ds):
+        ctx.solver, ctx.ds = solver, np.asarray(ds, dtype=np.float64)
+        return _like(interp(solver, _np(vc3)), vc3)
+
+    @staticmethod
+    def backward(ctx, grad_u):
+        sv = ctx.solver
+        hh = np.full(ctx.ds.shape, sv.lay.h0)
+        g = spread(sv, _np(grad_u), hh)
+        sv.set("DS", ctx.ds ** 3)                # restore the marker volumes
+        return _like(g, grad_u), None, None
+
+
+class MarkerSpread(torch.autograd.Function):
+    """f_E = spread(f_L); backward interpolates grad_fE and scales by ds^3 / hh^3."""
+
+    @staticmethod
+    def forward(ctx, f_l, solver, ds):
+        ctx.solver, ctx.ds = solver, np.asarray(ds, dtype=np.float64)
+        return _like(spread(solver, _np(f_l), ctx.ds), f_l)
+
+    @staticmethod
+    def backward(ctx, grad_fe):
+        sv = ctx.solver
+        u = interp(sv, _np(grad_fe))
+        scale = (ctx.ds ** 3 / sv.lay.h0 ** 3)[:, None]
+        return _like(u * scale, grad_fe), None, None

@@ -1,0 +1,85 @@
+"""Adjoint building blocks behind torch.autograd: transpose identities on the GPU kernels."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import parity_util as PU
+from pyib_b200 import _lib
+from pyib_b200 import autograd as AG
+from pyib_b200.device import DeviceSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(name="n3_osc"):
+    g = PU.golden(name)
+    lay = PU.layout_for(name)
+    sv = DeviceSolver(lay, rou=float(g["rou"]), visc=float(g["visc"]), cavity=bool(g["cavity"]),
+                      cg_max_iterations=5000)
+    sv.set_markers(g["ib_markers"], g["ib_vel"], g["ib_ds"])
+    return g, sv
+
+
+def _matvec(sv, z, dt):
+    sv.set("WORK_E", z)
+    sv.h.call("pyib_matvec", _lib.F["WORK_E"], _lib.F["WORK_E2"], C.c_double(dt), 1)
+    return sv.get("WORK_E2")
+
+
+def test_helmholtz_solve_adjoint_is_the_same_solve():
+    """<c, A^-1 d> through autograd equals <A^-1 c, d> and the exact <A y, z>.
+
+    d = A z and c = A y lie in the range of A (the closed cavity leaves a gauge
+    null space), so both solves have solutions; the CG stops at the reference's
+    relative tolerance, hence the 1e-6 bound.
+    """
+    g, sv = _solver()
+    dt = float(g["dt"])
+    free = sv.prec != 0.0
+    rng = np.random.default_rng(5)
+    z = rng.standard_normal(sv.lay.NE) * free
+    y = rng.standard_normal(sv.lay.NE) * free
+    d, c = _matvec(sv, z, dt), _matvec(sv, y, dt)
+    exact = float(np.dot(c, z))
+    d_t = torch.tensor(d, dtype=torch.float64, requires_grad=True)
+    s_t = torch.zeros(sv.lay.NE, dtype=torch.float64, requires_grad=True)
+    x = AG.HelmholtzSolve.apply(d_t, s_t, sv, dt)
+    loss = (torch.tensor(c) * x).sum()
+    loss.backward()
+    adjoint = float(torch.dot(d_t.grad, torch.tensor(d)))
+    assert abs(loss.item() - exact) <= 1e-6 * abs(exact)
+    assert abs(adjoint - exact) <= 1e-6 * abs(exact)
+    np.testing.assert_array_equal(s_t.grad.numpy(), c)       # d x / d s = identity
+    assert np.all(d_t.grad.numpy()[~free] == 0.0)
+
+
+def test_marker_interp_and_spread_are_transposes():
+    g, sv = _solver()
+    lay = sv.lay
+    rng = np.random.default_rng(7)
+    act = lay.cell_active
+    M = g["ib_markers"].shape[0]
+    ds = g["ib_ds"]
+    # interpolation: <interp(v), u> = <v, interp^T u>
+    v = torch.tensor(rng.standard_normal((3, lay.NC)) * act, dtype=torch.float64, requires_grad=True)
+    u = torch.tensor(rng.standard_normal((M, 3)), dtype=torch.float64)
+    out = AG.MarkerInterp.apply(v, sv, ds)
+    lhs = (out * u).sum()
+    lhs.backward()
+    rhs = (v.grad * v.detach()).sum()
+    assert abs(lhs.item() - rhs.item()) <= 1e-12 * abs(lhs.item())
+    # the forward matches the reference's interpolation of its golden field
+    vc = PU.cell3_to_dense("n3_osc", g["cv_vc"][:int(g["mesh_ncell"])])
+    assert PU.rel(AG.interp(sv, vc), g["ib_interp"]) < 1e-14
+    # spreading: <spread(f), h> = <f, spread^T h>
+    f = torch.tensor(rng.standard_normal((M, 3)), dtype=torch.float64, requires_grad=True)
+    h = torch.tensor(rng.standard_normal((3, lay.NC)) * act, dtype=torch.float64)
+    fe = AG.MarkerSpread.apply(f, sv, ds)
+    lhs = (fe * h).sum()
+    lhs.backward()
+    rhs = (f.grad * f.detach()).sum()
+    assert abs(lhs.item() - rhs.item()) <= 1e-12 * abs(lhs.item())
+    # the marker volumes are restored after an interpolation backward
+    np.testing.assert_array_equal(sv.get("DS"), ds ** 3)
