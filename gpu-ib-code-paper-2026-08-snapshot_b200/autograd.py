@@ -12,10 +12,12 @@ hand-written kernels as the forward path:
   Its transpose is spreading with ``hh^3`` in place of the marker volumes.
 * ``MarkerSpread``: ``f_E = sum w f_L ds^3`` (``ib_immersed.py:103-111``).  Its
   transpose is interpolation scaled by ``ds^3 / hh^3`` per marker.
+* ``MarkerInterpAt``: the interpolation at given marker positions, with the
+  gradient with respect to those positions through the delta-kernel weights
+  (``pyib_ib_interp_dx``, the per-marker 3x3 Jacobian).
 
-The stencil (cells and weights) is the one of the markers last set on the
-solver; derivatives with respect to marker positions (through the weights)
-are not part of these blocks.  Tensors are float64 in the solver's dense
+``MarkerInterp`` and ``MarkerSpread`` use the stencil of the markers last set
+on the solver.  Tensors are float64 in the solver's dense
 layout (edges: ``NE``; cell vectors: ``(3, NC)``; markers: ``(M, 3)``) on any
 device: they cross the C ABI as host arrays.
 """
@@ -118,3 +120,40 @@ class MarkerSpread(torch.autograd.Function):
         u = interp(sv, _np(grad_fe))
         scale = (ctx.ds ** 3 / sv.lay.h0 ** 3)[:, None]
         return _like(u * scale, grad_fe), None, None
+
+
+def interp_dx(solver, vc3):
+    """Per-marker Jacobian d u_L[m, c] / d x_m[d], shape (M, 3, 3), at the current markers."""
+    lay = solver.lay
+    full = np.zeros((3, lay.NC + solver.bfaces.size))
+    full[:, :lay.NC] = vc3
+    solver.set("VC", full)
+    _stencil(solver)
+    jac = np.empty(9 * solver.M)
+    solver.h.call("pyib_ib_interp_dx", jac.ctypes.data_as(C.POINTER(C.c_double)))
+    return jac.reshape(-1, 3, 3)
+
+
+class MarkerInterpAt(torch.autograd.Function):
+    """u_L = interp(vc) at ``markers`` (M, 3); gradients for vc and for the markers."""
+
+    @staticmethod
+    def forward(ctx, vc3, markers, solver, ds):
+        ds = np.asarray(ds, dtype=np.float64)
+        mk = _np(markers)
+        solver.set_markers(mk, np.zeros_like(mk), ds)
+        v = _np(vc3)
+        ctx.solver, ctx.ds, ctx.v, ctx.mk = solver, ds, v, mk
+        return _like(interp(solver, v), vc3)
+
+    @staticmethod
+    def backward(ctx, grad_u):
+        sv = ctx.solver
+        sv.set_markers(ctx.mk, np.zeros_like(ctx.mk), ctx.ds)   # the forward's positions
+        g = _np(grad_u)
+        jac = interp_dx(sv, ctx.v)
+        grad_mk = np.einsum("mc,mcd->md", g, jac)
+        hh = np.full(ctx.ds.shape, sv.lay.h0)
+        grad_vc = spread(sv, g, hh)
+        sv.set("DS", ctx.ds ** 3)
+        return _like(grad_vc, grad_u), _like(grad_mk, grad_u), None, None

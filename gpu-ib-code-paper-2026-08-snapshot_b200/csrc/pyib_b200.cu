@@ -119,6 +119,7 @@ struct pyib_ctx {
   double *mk = nullptr, *mvel = nullptr, *ds = nullptr, *fL = nullptr, *lag = nullptr,
          *dL = nullptr, *ibw = nullptr;
   int *ibcell = nullptr, *ibbase = nullptr;
+  double* ibjac = nullptr;        // 9 per marker: d u_L / d x_marker (pyib_ib_interp_dx)
   int *sort_keys_in = nullptr, *sort_keys_out = nullptr, *sort_vals_in = nullptr,
       *sort_vals_out = nullptr;
   void* sort_tmp = nullptr;
@@ -1214,6 +1215,59 @@ __global__ void k_ib_interp(int M, long long ncx, const int* __restrict__ cell, 
   }
 }
 
+// d/dr of delta_h3(r, h): the Roma-Peskin kernel is continuously differentiable
+// (the slope is -1/h^2 from both sides at |r| = h/2 and 0 at |r| = 3h/2)
+__device__ __forceinline__ double ddelta_h3(double r, double h) {
+  const double a = fabs(r / h);
+  double da;
+  if (a <= 0.5) {
+    const double t = 1.0 - (3.0 * a) * a;           // > 0 for a <= 1/2
+    da = -a / sqrt(t);
+  } else if (a <= 1.5) {
+    const double b = 1.0 - a;
+    const double t = 1.0 - 3.0 * (b * b);           // >= 1/4 for 1/2 < a <= 3/2
+    da = (-3.0 - 3.0 * b / sqrt(t)) / 6.0;
+  } else {
+    return 0.0;
+  }
+  return (r < 0.0 ? -da : da) / (h * h);
+}
+
+// Jacobian of the interpolation with respect to the marker positions:
+// jac[9 m + 3 c + d] = d u_L[m, c] / d x_m[d] = -hh^3 sum_o vc_c[cell_o] dw_o/dg_d, the
+// weight w_o = delta(gx) delta(gy) delta(gz) with g = node - marker (ib_immersed.py:63-93).
+// One thread per marker over the 125 offsets of its stencil base.
+__global__ void k_ib_interp_dx(int M, long long ncx, const double* __restrict__ mk, double px, double py,
+                               double pz, double dx, double hh, double hh3, int nx, int ny, int nz,
+                               const int* __restrict__ base, const double* __restrict__ vc, double* jac) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+    const double x = mk[3 * i], y = mk[3 * i + 1], z = mk[3 * i + 2];
+    const long long lx = base[3 * i], ly = base[3 * i + 1], lz = base[3 * i + 2];
+    double J[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int o = 0; o < 125; ++o) {
+      const long long ii = lx + (o / 25) - 2, jj = ly + ((o / 5) % 5) - 2, kk = lz + (o % 5) - 2;
+      if (!(ii >= 0 && ii < nx && jj >= 0 && jj < ny && kk >= 0 && kk < nz)) continue;
+      const double gx = (px + (double)ii * dx) - x;
+      const double gy = (py + (double)jj * dx) - y;
+      const double gz = (pz + (double)kk * dx) - z;
+      const double fx = delta_h3(gx, hh), fy = delta_h3(gy, hh), fz = delta_h3(gz, hh);
+      const double wx = -(ddelta_h3(gx, hh) * fy) * fz;
+      const double wy = -(fx * ddelta_h3(gy, hh)) * fz;
+      const double wz = -(fx * fy) * ddelta_h3(gz, hh);
+      const long long c = (kk * ny + jj) * nx + ii;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double v = vc[d * ncx + c] * hh3;
+        J[3 * d] += v * wx;
+        J[3 * d + 1] += v * wy;
+        J[3 * d + 2] += v * wz;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) jac[9 * i + q] = J[q];
+  }
+}
+
 __global__ void k_ib_keys(long long tot, const int* __restrict__ cell, const double* __restrict__ w,
                           int* keys, int* vals) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
@@ -1957,7 +2011,7 @@ int ib_alloc(pyib_ctx* ctx, int M) {
   if (ctx->M == M && ctx->mk) return PYIB_OK;
   void* ptrs[] = {ctx->mk, ctx->mvel, ctx->ds, ctx->fL, ctx->lag, ctx->dL, ctx->ibw, ctx->ibcell,
                   ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
-                  ctx->sort_vals_out, ctx->sort_tmp};
+                  ctx->sort_vals_out, ctx->sort_tmp, ctx->ibjac};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   ctx->M = M;
@@ -1971,6 +2025,7 @@ int ib_alloc(pyib_ctx* ctx, int M) {
   RET(alloc(ctx, (void**)&ctx->ibw, tot * sizeof(double)));
   RET(alloc(ctx, (void**)&ctx->ibcell, tot * sizeof(int)));
   RET(alloc(ctx, (void**)&ctx->ibbase, 3 * M * sizeof(int)));
+  RET(alloc(ctx, (void**)&ctx->ibjac, 9 * (long long)M * sizeof(double)));
   RET(alloc(ctx, (void**)&ctx->sort_keys_in, tot * sizeof(int)));
   RET(alloc(ctx, (void**)&ctx->sort_keys_out, tot * sizeof(int)));
   RET(alloc(ctx, (void**)&ctx->sort_vals_in, tot * sizeof(int)));
@@ -2216,7 +2271,7 @@ int pyib_destroy(pyib_ctx* ctx) {
                   ctx->ibcell, ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
                   ctx->sort_vals_out, ctx->sort_tmp, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
                   ctx->vcm32, ctx->vq32, ctx->prec32, ctx->pa_val32, ctx->pv_val32,
-                  ctx->pr_val32, ctx->diag1, ctx->diag2};
+                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->ibjac};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
@@ -2438,6 +2493,20 @@ int pyib_ib_interp(pyib_ctx* ctx) {
   if (!ctx) return PYIB_E_ARG;
   if (!ctx->stencil_valid) RET(ib_stencil(ctx));
   RET(ib_interp(ctx, ctx->lag));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PYIB_OK;
+}
+
+int pyib_ib_interp_dx(pyib_ctx* ctx, double* jac) {
+  if (!ctx || !jac) return PYIB_E_ARG;
+  if (ctx->M <= 0) return set_err(ctx, PYIB_E_STATE, "no markers");
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->stencil_valid) RET(ib_stencil(ctx));
+  k_ib_interp_dx<<<grid_for(ctx->M), kThreads, 0, ctx->stream>>>(
+      ctx->M, ncx_of(ctx), ctx->mk, ctx->pos_ref[0], ctx->pos_ref[1], ctx->pos_ref[2], ctx->dx, ctx->prm.hh,
+      ctx->prm.hh3, ctx->ib_n[0], ctx->ib_n[1], ctx->ib_n[2], ctx->ibbase, ctx->vc, ctx->ibjac);
+  CKL();
+  CK(cudaMemcpyAsync(jac, ctx->ibjac, 9 * (size_t)ctx->M * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return PYIB_OK;
 }

@@ -200,6 +200,11 @@ int pyib_ib_interp(pyib_ctx* ctx);
 /* Lagrangian -> Eulerian: FE = spread(FL) with ds^3 weights (_spread_stencil,
  * 103-111).  Deterministic: contributions sorted by cell, summed in input order. */
 int pyib_ib_spread(pyib_ctx* ctx);
+/* Derivative of the interpolation with respect to the marker positions, for adjoint
+ * gradients: jac[9*m + 3*c + d] = d u_L[m, c] / d x_m[d] (M*9 doubles, host buffer) at
+ * the current markers and PYIB_F_VC.  The derivative of ImmersedBoundary's weights
+ * and interpolation (ib_immersed.py:12-19, 63-93); the reference has no derivative. */
+int pyib_ib_interp_dx(pyib_ctx* ctx, double* jac);
 
 /* ---- loads (ib_interior.py) ------------------------------------------------- */
 /* ClosedSphereLoadCorrection.evaluate + fluid force/moment integrals

@@ -83,3 +83,40 @@ def test_marker_interp_and_spread_are_transposes():
     assert abs(lhs.item() - rhs.item()) <= 1e-12 * abs(lhs.item())
     # the marker volumes are restored after an interpolation backward
     np.testing.assert_array_equal(sv.get("DS"), ds ** 3)
+
+
+def test_marker_position_gradient_matches_finite_differences():
+    """d/dx of sum(w * interp(vc) at markers x) against a central difference.
+
+    The Roma-Peskin kernel is continuously differentiable, so the difference
+    along a random direction converges to the kernel's Jacobian (step 1e-6 h).
+    """
+    g, sv = _solver()
+    rng = np.random.default_rng(9)
+    vc = PU.cell3_to_dense("n3_osc", g["cv_vc"][:int(g["mesh_ncell"])])
+    mk0, ds = np.asarray(g["ib_markers"]), g["ib_ds"]
+    w = rng.standard_normal(mk0.shape)
+    vc_t = torch.tensor(vc, dtype=torch.float64)
+    mk_t = torch.tensor(mk0, dtype=torch.float64, requires_grad=True)
+    u = AG.MarkerInterpAt.apply(vc_t, mk_t, sv, ds)
+    (u * torch.tensor(w)).sum().backward()
+    ad_grad = mk_t.grad.numpy().copy()
+
+    def f(mk):
+        return float((AG.MarkerInterpAt.apply(vc_t, torch.tensor(mk), sv, ds).numpy() * w).sum())
+
+    direction = rng.standard_normal(mk0.shape)
+    eps = 1e-6 * sv.lay.h0
+    fd = (f(mk0 + eps * direction) - f(mk0 - eps * direction)) / (2.0 * eps)
+    ad = float(np.sum(ad_grad * direction))
+    assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+    # per marker: the Jacobian of one marker's velocity along x
+    m, c = 3, 0
+    e = np.zeros_like(mk0)
+    e[m, 0] = 1.0
+    fp = AG.MarkerInterpAt.apply(vc_t, torch.tensor(mk0 + eps * e), sv, ds).numpy()[m, c]
+    fm = AG.MarkerInterpAt.apply(vc_t, torch.tensor(mk0 - eps * e), sv, ds).numpy()[m, c]
+    sv.set_markers(mk0, np.zeros_like(mk0), ds)
+    jac = AG.interp_dx(sv, vc)
+    assert abs((fp - fm) / (2.0 * eps) - jac[m, c, 0]) <= 1e-5 * np.max(np.abs(jac[m])) + 1e-12
+
