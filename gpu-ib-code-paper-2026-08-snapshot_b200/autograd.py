@@ -15,6 +15,13 @@ hand-written kernels as the forward path:
 * ``MarkerInterpAt``: the interpolation at given marker positions, with the
   gradient with respect to those positions through the delta-kernel weights
   (``pyib_ib_interp_dx``, the per-marker 3x3 Jacobian).
+* ``MarkerSpreadAt``: spreading at given marker positions; its position gradient
+  is the interpolation Jacobian of the incoming gradient field, scaled by
+  ``ds^3 / hh^3`` and contracted with the marker forces.
+* ``CalcVel``: the cell velocity of ``Driver.calc_vel`` (``ib_driver_np.py:267-291``),
+  ``vc = P C s`` with the inlet edges of s replaced by their prescribed values.
+  Its transpose is ``R I (vol * g)`` (``R = C^T``; the interpolation ``P`` is the
+  integration ``I`` weighted by the cell volume factor), zero on inlet edges.
 
 ``MarkerInterp`` and ``MarkerSpread`` use the stencil of the markers last set
 on the solver.  Tensors are float64 in the solver's dense
@@ -157,3 +164,58 @@ class MarkerInterpAt(torch.autograd.Function):
         grad_vc = spread(sv, g, hh)
         sv.set("DS", ctx.ds ** 3)
         return _like(grad_vc, grad_u), _like(grad_mk, grad_u), None, None
+
+
+class MarkerSpreadAt(torch.autograd.Function):
+    """f_E = spread(f_L) at ``markers``; gradients for f_L and for the markers."""
+
+    @staticmethod
+    def forward(ctx, f_l, markers, solver, ds):
+        ds = np.asarray(ds, dtype=np.float64)
+        mk = _np(markers)
+        solver.set_markers(mk, np.zeros_like(mk), ds)
+        f = _np(f_l)
+        ctx.solver, ctx.ds, ctx.mk, ctx.f = solver, ds, mk, f
+        return _like(spread(solver, f, ds), f_l)
+
+    @staticmethod
+    def backward(ctx, grad_fe):
+        sv = ctx.solver
+        sv.set_markers(ctx.mk, np.zeros_like(ctx.mk), ctx.ds)   # the forward's positions
+        g = _np(grad_fe)
+        scale = (ctx.ds ** 3 / sv.lay.h0 ** 3)[:, None]
+        grad_f = interp(sv, g) * scale
+        jac = interp_dx(sv, g)
+        grad_mk = np.einsum("mc,mcd->md", ctx.f, jac) * scale
+        return _like(grad_f, grad_fe), _like(grad_mk, grad_fe), None, None
+
+
+def calc_vel(solver, s):
+    """Cell velocity (3, NC) of ``s`` (the inlet edges take their prescribed values)."""
+    solver.set("S", s)
+    solver.h.call("pyib_calc_vel")
+    return solver.vc_cells()
+
+
+def calc_vel_transpose(solver, g):
+    """s-gradient (NE) of sum(g * calc_vel(s)): R I (vol * g), zero on inlet edges."""
+    solver.set("WORK_C3", np.asarray(g, dtype=np.float64) * solver.ops.vol_ci[None, :])
+    solver.h.call("pyib_operator", 3)        # integr_c2f: WORK_C3 -> WORK_F
+    solver.h.call("pyib_operator", 1)        # rot: WORK_F -> WORK_E
+    out = solver.get("WORK_E")
+    out[solver.inlet] = 0.0
+    return out
+
+
+class CalcVel(torch.autograd.Function):
+    """vc = calc_vel(s) on the active cells; backward applies its transpose."""
+
+    @staticmethod
+    def forward(ctx, s, solver):
+        ctx.solver = solver
+        return _like(calc_vel(solver, _np(s)), s)
+
+    @staticmethod
+    def backward(ctx, grad_vc):
+        return _like(calc_vel_transpose(ctx.solver, _np(grad_vc)), grad_vc), None
+

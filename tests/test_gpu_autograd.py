@@ -120,3 +120,48 @@ def test_marker_position_gradient_matches_finite_differences():
     jac = AG.interp_dx(sv, vc)
     assert abs((fp - fm) / (2.0 * eps) - jac[m, c, 0]) <= 1e-5 * np.max(np.abs(jac[m])) + 1e-12
 
+
+
+@pytest.mark.parametrize("name", ["n3_osc", "n2_fixed"])
+def test_calc_vel_transpose(name):
+    """<calc_vel(s) - calc_vel(0), g> = <s, calc_vel^T g>; the inflow case is affine
+    (its inlet edges take prescribed values), the cavity case linear."""
+    g, sv = _solver(name)
+    lay = sv.lay
+    rng = np.random.default_rng(11)
+    s = rng.standard_normal(lay.NE) * lay.edge_exists
+    gv = rng.standard_normal((3, lay.NC)) * lay.cell_active
+    s_t = torch.tensor(s, dtype=torch.float64, requires_grad=True)
+    vc = AG.CalcVel.apply(s_t, sv)
+    base = AG.calc_vel(sv, np.zeros(lay.NE))
+    lhs = float(((vc.detach().numpy() - base) * gv).sum())
+    (vc * torch.tensor(gv)).sum().backward()
+    rhs = float((s_t.grad.numpy() * s).sum())
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (lhs, rhs)
+    assert np.all(s_t.grad.numpy()[sv.inlet] == 0.0)
+
+
+def test_marker_spread_position_gradient_matches_finite_differences():
+    g, sv = _solver()
+    lay = sv.lay
+    rng = np.random.default_rng(13)
+    mk0, ds = np.asarray(g["ib_markers"]), g["ib_ds"]
+    f = rng.standard_normal(mk0.shape)
+    # a smooth weight field: the reference's own cell velocity
+    h = PU.cell3_to_dense("n3_osc", g["cv_vc"][:int(g["mesh_ncell"])])
+    f_t = torch.tensor(f, dtype=torch.float64, requires_grad=True)
+    mk_t = torch.tensor(mk0, dtype=torch.float64, requires_grad=True)
+    fe = AG.MarkerSpreadAt.apply(f_t, mk_t, sv, ds)
+    (fe * torch.tensor(h)).sum().backward()
+    ad_mk, ad_f = mk_t.grad.numpy().copy(), f_t.grad.numpy().copy()
+
+    def loss(mk, ff):
+        return float((AG.MarkerSpreadAt.apply(torch.tensor(ff), torch.tensor(mk), sv, ds).numpy() * h).sum())
+
+    direction = rng.standard_normal(mk0.shape)
+    eps = 1e-6 * lay.h0
+    fd = (loss(mk0 + eps * direction, f) - loss(mk0 - eps * direction, f)) / (2.0 * eps)
+    ad = float(np.sum(ad_mk * direction))
+    assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+    # linear in the forces: the gradient is exact
+    assert abs(loss(mk0, f) - float(np.sum(ad_f * f))) <= 1e-12 * abs(loss(mk0, f))
