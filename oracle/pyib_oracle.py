@@ -262,6 +262,30 @@ class IBStencil:
         fl = (vel - self.interp(vc, st)) / dt
         return self.spread(fl, st, ds), fl
 
+    def coupling_matrix(self, stencil, ds, reg=1e-8):
+        """M = D S + reg tr(M)/nmk I, ib_immersed.py:122-146.
+
+        D[i, c] = sum_k w_ik hh^3 [cell_ik = c] (interpolation), S[c, j] = sum_k
+        w_jk ds_j^3 [cell_jk = c] (spreading); dense nmk x nmk.
+        """
+        import scipy.sparse as sp
+        cell, w = stencil
+        nmk = cell.shape[0]
+        rows = np.repeat(np.arange(nmk), cell.shape[1])
+        cols = cell.ravel()
+        D = sp.csr_matrix(((w * self.hh ** 3).ravel(), (rows, cols)), shape=(nmk, self.ncell))
+        S = sp.csr_matrix(((w * (np.asarray(ds) ** 3)[:, None]).ravel(), (cols, rows)), shape=(self.ncell, nmk))
+        M = np.asarray((D @ S).todense())
+        M += reg * np.trace(M) / nmk * np.eye(nmk)
+        return M
+
+    def implicit_force(self, vc, markers, vel, dt, ds):   # ib_immersed.py:154-174
+        """Solve M f = (vel - interp(vc))/dt with the coupling matrix; F_E = spread(f)."""
+        st = self.build(markers)
+        rhs = (vel - self.interp(vc, st)) / dt
+        f = np.linalg.inv(self.coupling_matrix(st, ds)) @ rhs
+        return self.spread(f, st, ds), f
+
 
 # ---------------------------------------------------------------------------
 # kinematics and closed-sphere loads
@@ -384,7 +408,14 @@ class OracleDriver:
         self.last_stats = []
 
     # -- IB wiring (ib_driver_np.py:179-201, 241-249)
-    def set_ib(self, stencil: IBStencil, markers, ds, vel):
+    def set_ib(self, stencil: IBStencil, markers, ds, vel, force_mode="accumulated_explicit", implicit=False,
+               alpha=1.0):
+        """force_mode: "accumulated_explicit" (ib_driver_np.py:447-451, 511-525) or
+        "replacement" (the public "direct": the force of every inner iteration replaces
+        the last one, scaled by alpha, explicit or implicit, ib_driver_np.py:466-486)."""
+        if force_mode not in ("accumulated_explicit", "replacement"):
+            raise ValueError(force_mode)
+        self.force_mode, self.implicit, self.alpha = force_mode, bool(implicit), float(alpha)
         self.ib = stencil
         self.markers = np.asarray(markers, dtype=np.float64)
         self.ds = np.asarray(ds, dtype=np.float64)
@@ -485,10 +516,12 @@ class OracleDriver:
         rou, ac, ad = self.rou, self.ac, self.ad
         self.time += dt
         stats = []
+        accumulated = self.ib is None or self.force_mode == "accumulated_explicit"
         if self.ib is not None and self.motion is not None:
             self.markers, self.vel = self.motion(self.time)
-            st = self.ib.build(self.markers)
-            self.fE = self.ib.spread(self.fL, st, self.ds)
+            if accumulated:
+                st = self.ib.build(self.markers)
+                self.fE = self.ib.spread(self.fL, st, self.ds)
         _, U, vc = self.calc_vel(s)
         conv0, diff0 = self.conv_diff(U, vc)
         res0 = rou * vc[:nc] - (1 - ac) * dt * rou * conv0 + (1 - ad) * dt * diff0
@@ -501,6 +534,12 @@ class OracleDriver:
             conv, diff = self.conv_diff(U, vc)
             res = res0 - rou * vc[:nc] - ac * dt * rou * conv + ad * dt * diff
             if self.ib is not None:
+                if not accumulated:
+                    # the force of this inner iteration replaces the last (ib_driver_np.py:466-486)
+                    force = self.ib.implicit_force if self.implicit else self.ib.direct_force
+                    fE, fL = force(vc[:nc], self.markers, self.vel, dt, self.ds)
+                    self.fE = (rou * self.alpha) * fE
+                    self.fL = (rou * self.alpha) * fL
                 res = res + dt * self.fE
             if it == inner:
                 self.last_res = res
@@ -508,7 +547,7 @@ class OracleDriver:
             s, st = self.helm_solve(res_e, s, dt)
             stats.append(st)
             s, U, vc = self.calc_vel(s)
-            if self.ib is not None and it == 1:
+            if self.ib is not None and accumulated and it == 1:
                 dE, dL = self.ib.direct_force(vc[:nc], self.markers, self.vel, dt, self.ds)
                 self.fE = self.fE + rou * dE
                 self.fL = self.fL + rou * dL
