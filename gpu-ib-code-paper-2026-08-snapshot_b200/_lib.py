@@ -65,7 +65,8 @@ class Params(C.Structure):
         ("cavity", C.c_int32), ("check", C.c_int32), ("cg_max", C.c_int32), ("strict", C.c_int32),
         ("precision", C.c_int32), ("nmarkers", C.c_int32),
         ("hh", C.c_double), ("hh3", C.c_double),
-        ("mixed_tol", C.c_double), ("mixed_max_sweeps", C.c_int32), ("pad", C.c_int32),
+        ("mixed_tol", C.c_double), ("mixed_max_sweeps", C.c_int32), ("ib_mode", C.c_int32),
+        ("ib_alpha", C.c_double),
     ]
 
 

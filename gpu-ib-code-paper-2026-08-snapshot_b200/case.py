@@ -182,10 +182,21 @@ def validate_config(raw: dict) -> dict:
     ib = cfg["ib"]
     ib["radius"] = _positive("ib.radius", ib["radius"])
     ib["marker_spacing"] = _positive("ib.marker_spacing", ib["marker_spacing"])
-    if ib["force_mode"] != "accumulated_explicit" or ib["implicit"] or float(ib["alpha"]) != 1.0:
-        raise CaseConfigError("the b200 device runs accumulated_explicit forcing with alpha=1, explicit")
-    if tm["inner_iterations"] < 2:
-        raise CaseConfigError("accumulated_explicit requires at least two fluid inner iterations")
+    # IB force mode, as ib_case.py:354-371 validates it
+    if ib["force_mode"] not in ("direct", "accumulated_explicit"):
+        raise CaseConfigError("ib.force_mode must be 'accumulated_explicit' or 'direct'")
+    if not isinstance(ib["implicit"], (bool, np.bool_)):
+        raise CaseConfigError("ib.implicit must be a boolean")
+    ib["alpha"] = _positive("ib.alpha", ib["alpha"])
+    if ib["force_mode"] == "accumulated_explicit":
+        if ib["implicit"]:
+            raise CaseConfigError("accumulated_explicit is an explicit IB method")
+        if ib["alpha"] != 1.0:
+            raise CaseConfigError("accumulated_explicit requires ib.alpha=1.0")
+        if tm["inner_iterations"] < 2:
+            raise CaseConfigError("accumulated_explicit requires at least two fluid inner iterations")
+    elif ib["implicit"] and ib["alpha"] > 0.7:
+        raise CaseConfigError("implicit IB currently requires ib.alpha <= 0.7")
     mo = ib["motion"]
     expected = {"fixed_sphere": "none", "oscillating_sphere": "oscillation", "rotating_sphere": "rotation"}[kind]
     if mo["kind"] != expected:
@@ -289,6 +300,9 @@ def build_runtime(cfg) -> CaseRuntime:
     drv.cg_check_interval = so["cg_check_interval"]
     if cfg["mesh"]["kind"] in {"sphere_concentric", "nested_boxes"}:
         drv.set_cavity(U_lid=0.0, spanwise_zerograd=False)
+    fm = "replacement" if ib["force_mode"] == "direct" else "accumulated_explicit"
+    drv.ib_implicit = bool(ib["implicit"])
+    drv.ib_alpha = float(ib["alpha"])
     count = max(12, int(round(4.0 * np.pi * radius ** 2 / ib["marker_spacing"] ** 2)))
     markers = fibonacci_sphere(count, radius, centre)
     width = (4.0 * np.pi * radius ** 2 * dx / count) ** (1.0 / 3.0)
@@ -297,13 +311,13 @@ def build_runtime(cfg) -> CaseRuntime:
     if mo["kind"] == "oscillation":
         motion = Oscillation(markers, mo["axis"], mo["amplitude"], mo["frequency"], mo["phase"])
         mk0, v0 = motion(0.0)
-        drv.set_ib(None, mk0, ds, v0)
+        drv.set_ib(None, mk0, ds, v0, force_mode=fm)
         drv.set_motion(motion, 0.0)
     elif mo["kind"] == "rotation":
         omega = np.asarray(mo["axis"]) * mo["spin_ratio"] * uref / radius
-        drv.set_ib(None, markers, ds, np.cross(omega, markers - centre))
+        drv.set_ib(None, markers, ds, np.cross(omega, markers - centre), force_mode=fm)
     else:
-        drv.set_ib(None, markers, ds, np.zeros_like(markers))
+        drv.set_ib(None, markers, ds, np.zeros_like(markers), force_mode=fm)
     loads = SphereLoads(drv, centre, exc, radius, dx, rho, 1.5 * dx)
     return CaseRuntime(config=cfg, layout=lay, driver=drv, loads=loads, motion=motion, dx=dx,
                        dt=cfg["time"]["dt"], steps=cfg["time"]["steps"],
@@ -401,7 +415,7 @@ def load_checkpoint(path: Path, rt: CaseRuntime):
         rt.loads.current = np.asarray(d["loads"])
         if rt.motion is not None:
             mk, v = rt.motion(drv.time)
-            drv.set_ib(drv.ib, mk, drv.ib_ds, v)
+            drv.set_ib(drv.ib, mk, drv.ib_ds, v, force_mode=drv.ib_force_mode)
     return step, s, s_old
 
 

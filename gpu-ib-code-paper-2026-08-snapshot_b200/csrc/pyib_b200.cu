@@ -120,6 +120,7 @@ struct pyib_ctx {
          *dL = nullptr, *ibw = nullptr;
   int *ibcell = nullptr, *ibbase = nullptr;
   double* ibjac = nullptr;        // 9 per marker: d u_L / d x_marker (pyib_ib_interp_dx)
+  int imp_iters = 0;              // CG iterations of the last implicit IB solve
   int *sort_keys_in = nullptr, *sort_keys_out = nullptr, *sort_vals_in = nullptr,
       *sort_vals_out = nullptr;
   void* sort_tmp = nullptr;
@@ -1309,6 +1310,23 @@ __global__ void k_ib_force(int M, const double* __restrict__ vel, const double* 
     dL[q] = (vel[q] - uL[q]) / dt;
 }
 
+// y = a * x  (the direct force mode's replacement, ib_driver_np.py:480-481)
+__global__ void k_set_scaled(long long n, double* y, double a, const double* __restrict__ x) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    y[q] = a * x[q];
+}
+
+// trace of the marker coupling matrix: sum_i ds_i^3 sum_k w_ik^2 (times hh^3 on the host)
+__global__ void __launch_bounds__(kThreads) k_ib_trace(long long tot, const double* __restrict__ w,
+                                                       const double* __restrict__ ds3, double* partials,
+                                                       CGState* st, double* out) {
+  double v[1] = {0.0};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x)
+    v[0] += (w[t] * w[t]) * ds3[t / 125];
+  if (grid_sum<1>(v, partials, &st->counter)) *out = v[0];
+}
+
 __global__ void k_axpy_scaled(long long n, double* y, double a, const double* x) {
   // y = y + (a * x)  (ib_driver_np.py:522-525)
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
@@ -2007,6 +2025,78 @@ int ib_spread(pyib_ctx* ctx, const double* f, double* out) {
   return PYIB_OK;
 }
 
+// Implicit direct forcing (ib_immersed.py:122-174): f solves (D S + eps I) f = rhs,
+// D = interpolation (w hh^3), S = spreading (w ds^3), eps = 1e-8 tr(D S)/M.  With
+// sq = sqrt(ds^3) the system is the symmetric positive definite
+//   sq * D S (y / sq) + eps y = sq * rhs,   f = y / sq,
+// solved by CG: the operator applies the device spreading and interpolation, the
+// 3M-long marker vectors (the three components as one block-diagonal system) stay
+// on the host, where the dot products are plain sequential sums.  rhs and the
+// result are in ctx->dL; ctx->lag and ctx->conv are scratch.
+int ib_implicit_solve(pyib_ctx* ctx) {
+  const int M = ctx->M;
+  const long long n = 3LL * M, nc = ctx->lay.ncell, tot = (long long)M * 125;
+  std::vector<double> ds3(M), b(n), y(n, 0.0), r(n), p(n), ap(n), tmp(n);
+  CK(cudaMemcpyAsync(ds3.data(), ctx->ds, M * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(b.data(), ctx->dL, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  double* dtr = ctx->partials + (size_t)(kSlots - 2) * kPartStride;   // one double of scratch
+  k_ib_trace<<<grid_for(tot), kThreads, 0, ctx->stream>>>(tot, ctx->ibw, ctx->ds, ctx->partials, ctx->st, dtr);
+  CKL();
+  double trace = 0.0;
+  CK(cudaMemcpyAsync(&trace, dtr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const double eps = 1e-8 * (trace * ctx->prm.hh3) / M;
+  std::vector<double> sq(M);
+  for (int i = 0; i < M; ++i) sq[i] = std::sqrt(ds3[i]);
+  auto apply = [&](const std::vector<double>& in, std::vector<double>& out) -> int {
+    for (long long q = 0; q < n; ++q) tmp[q] = in[q] / sq[q / 3];
+    CK(cudaMemcpyAsync(ctx->lag, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    RET(ib_spread(ctx, ctx->lag, ctx->conv));
+    k_ib_interp<<<grid_for(M), kThreads, 0, ctx->stream>>>(M, nc, ctx->ibcell, ctx->ibw, ctx->prm.hh3, ctx->conv,
+                                                          ctx->dL);
+    CKL();
+    CK(cudaMemcpyAsync(out.data(), ctx->dL, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (long long q = 0; q < n; ++q) out[q] = sq[q / 3] * out[q] + eps * in[q];
+    return PYIB_OK;
+  };
+  double bb = 0.0;
+  for (long long q = 0; q < n; ++q) {
+    b[q] *= sq[q / 3];
+    r[q] = b[q];
+    p[q] = b[q];
+    bb += b[q] * b[q];
+  }
+  double rr = bb;
+  const double target = 1e-26 * bb;           // |r| <= 1e-13 |b|
+  int it = 0;
+  const int max_it = 2000;
+  while (rr > target && it < max_it) {
+    RET(apply(p, ap));
+    double pap = 0.0;
+    for (long long q = 0; q < n; ++q) pap += p[q] * ap[q];
+    if (!(pap > 0.0)) return set_err(ctx, PYIB_E_NOCONV, "implicit IB solve: coupling matrix not positive");
+    const double alpha = rr / pap;
+    double rr_new = 0.0;
+    for (long long q = 0; q < n; ++q) {
+      y[q] += alpha * p[q];
+      r[q] -= alpha * ap[q];
+      rr_new += r[q] * r[q];
+    }
+    const double beta = rr_new / rr;
+    for (long long q = 0; q < n; ++q) p[q] = r[q] + beta * p[q];
+    rr = rr_new;
+    ++it;
+  }
+  if (!(rr <= target))
+    return set_err(ctx, PYIB_E_NOCONV, "implicit IB solve did not converge: %d iterations, |r|/|b| = %.3e", it,
+                   std::sqrt(rr / (bb > 0.0 ? bb : 1.0)));
+  for (long long q = 0; q < n; ++q) tmp[q] = y[q] / sq[q / 3];
+  CK(cudaMemcpyAsync(ctx->dL, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->imp_iters = it;
+  return PYIB_OK;
+}
+
 int ib_alloc(pyib_ctx* ctx, int M) {
   if (ctx->M == M && ctx->mk) return PYIB_OK;
   void* ptrs[] = {ctx->mk, ctx->mvel, ctx->ds, ctx->fL, ctx->lag, ctx->dL, ctx->ibw, ctx->ibcell,
@@ -2044,7 +2134,10 @@ int ib_alloc(pyib_ctx* ctx, int M) {
 int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* markers,
             const double* vel, pyib_step_stats* out) {
   if (!tables_ready(ctx) || !ctx->have_params) return set_err(ctx, PYIB_E_STATE, "context not ready");
-  if (inner < 2) return set_err(ctx, PYIB_E_ARG, "accumulated_explicit requires at least 2 fluid inner iterations");
+  const bool accumulated = ctx->prm.ib_mode == 0;
+  if (accumulated && inner < 2)
+    return set_err(ctx, PYIB_E_ARG, "accumulated_explicit requires at least 2 fluid inner iterations");
+  if (inner < 1) return set_err(ctx, PYIB_E_ARG, "at least one fluid inner iteration");
   const pyib_params& P = ctx->prm;
   const long long nc = ctx->lay.ncell, ne = ctx->lay.nedge;
   const bool ib = ctx->M > 0;
@@ -2054,7 +2147,7 @@ int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* ma
     CK(cudaMemcpyAsync(ctx->mk, markers, 3 * ctx->M * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->mvel, vel, 3 * ctx->M * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     RET(ib_stencil(ctx));
-    RET(ib_spread(ctx, ctx->fL, ctx->fE));        // held force follows the body (ib_driver_np.py:447-451)
+    if (accumulated) RET(ib_spread(ctx, ctx->fL, ctx->fE));   // held force follows the body (ib_driver_np.py:447-451)
   } else if (ib && !ctx->stencil_valid) {
     RET(ib_stencil(ctx));
   }
@@ -2065,6 +2158,20 @@ int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* ma
   CKL();
   RET(op_calc_vel(ctx));
   for (int it = 1; it <= inner; ++it) {
+    if (ib && !accumulated) {
+      // direct mode: this iteration's force replaces the last (ib_driver_np.py:466-486)
+      RET(ib_interp(ctx, ctx->lag));
+      k_ib_force<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(ctx->M, ctx->mvel, ctx->lag, dt, ctx->dL);
+      CKL();
+      if (ctx->prm.ib_mode == 2) RET(ib_implicit_solve(ctx));
+      RET(ib_spread(ctx, ctx->dL, ctx->conv));   // conv is free scratch before op_convdiff
+      const double ra = rou * ctx->prm.ib_alpha;
+      k_set_scaled<<<grid_for(3 * nc), kThreads, 0, ctx->stream>>>(3 * nc, ctx->fE, ra, ctx->conv);
+      CKL();
+      k_set_scaled<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(3 * ctx->M, ctx->fL, ra, ctx->dL);
+      CKL();
+      st.ib_updates += 1;
+    }
     RET(op_convdiff(ctx, 2, (ac * dt) * rou, ad * dt, dt, ctx->res_c0, ib ? ctx->fE : nullptr, ctx->res_c,
                     nullptr));
     RET(op_integr(ctx, ctx->res_c, nc, ctx->F));
@@ -2079,7 +2186,7 @@ int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* ma
     if (out) *out = st;
     if (rc != PYIB_OK) return rc;
     RET(op_calc_vel(ctx));
-    if (ib && it == 1) {
+    if (ib && accumulated && it == 1) {
       RET(ib_interp(ctx, ctx->lag));
       k_ib_force<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(ctx->M, ctx->mvel, ctx->lag, dt, ctx->dL);
       CKL();
@@ -2353,6 +2460,8 @@ int pyib_set_params(pyib_ctx* ctx, const pyib_params* p) {
     ctx->mix_graph_check = -1;
   }
   if (p->precision != 0 && p->precision != 1) return set_err(ctx, PYIB_E_ARG, "precision must be 0 or 1");
+  if (p->ib_mode < 0 || p->ib_mode > 2) return set_err(ctx, PYIB_E_ARG, "ib_mode must be 0, 1 or 2");
+  if (p->ib_mode != 0 && !(p->ib_alpha > 0.0)) return set_err(ctx, PYIB_E_ARG, "ib_alpha must be positive");
   if (p->nmarkers > 0) RET(ib_alloc(ctx, p->nmarkers));
   return PYIB_OK;
 }

@@ -158,7 +158,8 @@ class DeviceSolver:
 
     def __init__(self, lay: NestedLayout, *, rou, visc, cavity, cg_check_interval=20,
                  cg_max_iterations=1000, strict=False, ac=0.5, ad=0.5, tol1=1e-10, tol2=1e-9,
-                 device=0, precision="float64", mixed_tol=0.1, mixed_max_sweeps=200, tables=None):
+                 device=0, precision="float64", mixed_tol=0.1, mixed_max_sweeps=200, tables=None,
+                 ib_mode=0, ib_alpha=1.0):
         if tables is None:
             tables = LayoutTables(lay, cavity)
         elif tables.lay is not lay or tables.cavity != bool(cavity):
@@ -195,7 +196,8 @@ class DeviceSolver:
                            cg_max=int(cg_max_iterations), strict=int(bool(strict)),
                            precision={"float64": 0, "mixed": 1}[precision],
                            nmarkers=0, hh=lay.h0, hh3=lay.h0 ** 3, mixed_tol=float(mixed_tol),
-                           mixed_max_sweeps=int(mixed_max_sweeps))
+                           mixed_max_sweeps=int(mixed_max_sweeps), ib_mode=int(ib_mode),
+                           ib_alpha=float(ib_alpha))
         self._push_params()
         pos_ref = (lay.levels[0].lo + 0.5 * lay.h0).astype(np.float64)
         self.pos_ref = pos_ref

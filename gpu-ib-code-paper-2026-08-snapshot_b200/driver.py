@@ -76,7 +76,9 @@ class B200Driver:
         self.helmholtz_total_iterations_last_step = 0
         self.ib_force_updates_last_step = 0
         self.ib_force_update_count = 0
-        self.ib_implicit = False
+        self.ib_implicit = False       # force_mode "replacement": solve M f = rhs (implicit_force)
+        self.ib_alpha = 1.0            # force_mode "replacement": relaxation of the replaced force
+        self.ib_force_mode = "accumulated_explicit"
         self.last_step_dt = None
         self.last_helm_m = 0
         self._tables = tables          # shared LayoutTables of this layout (optional)
@@ -91,11 +93,18 @@ class B200Driver:
         return self
 
     def set_ib(self, ib, markers, ds, vel_desired, force_mode="accumulated_explicit"):
-        """Attach the body (ib_driver_np.py:179-201); accumulated explicit forcing only."""
-        if force_mode not in ("accumulated_explicit", "fortran_accumulated"):
-            raise ValueError(f"unsupported IB force_mode on b200: {force_mode!r}")
+        """Attach the body (ib_driver_np.py:179-201).
+
+        ``accumulated_explicit`` (alias ``fortran_accumulated``): one explicit force
+        increment per step, held and carried with the body.  ``replacement`` (the
+        public ``direct``): the force of every inner iteration replaces the last,
+        scaled by ``ib_alpha``, explicit or, with ``ib_implicit``, solved with the
+        marker coupling matrix.
+        """
+        if force_mode not in ("accumulated_explicit", "fortran_accumulated", "replacement"):
+            raise ValueError(f"unsupported IB force_mode: {force_mode!r}")
         self.ib = ib if ib is not None else True
-        self.ib_force_mode = "accumulated_explicit"
+        self.ib_force_mode = "replacement" if force_mode == "replacement" else "accumulated_explicit"
         self._markers = np.asarray(markers, dtype=np.float64).reshape(-1, 3)
         self._vel = np.asarray(vel_desired, dtype=np.float64).reshape(-1, 3)
         self._ds = np.asarray(ds, dtype=np.float64).reshape(-1)
@@ -124,8 +133,10 @@ class B200Driver:
                                         and self._tables.cavity == self.cavity else None)
             self._ib_dirty = True
         sv = self._solver
+        mode = 0 if self.ib_force_mode == "accumulated_explicit" else (2 if self.ib_implicit else 1)
         want = dict(check=int(self.cg_check_interval), cg_max=int(self.cg_max_iterations),
-                    strict=int(bool(self.fail_on_cg_nonconvergence)))
+                    strict=int(bool(self.fail_on_cg_nonconvergence)), ib_mode=mode,
+                    ib_alpha=float(self.ib_alpha))
         if any(sv.params[k] != v for k, v in want.items()):
             sv.params.update(want)
             sv._push_params()

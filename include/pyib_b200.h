@@ -73,7 +73,11 @@ typedef struct pyib_params {
   double mixed_tol;          /* precision 1: inner float32 solve reduces the
                                 preconditioned residual norm by this factor      */
   int32_t mixed_max_sweeps;  /* precision 1: cap on float64 refinement sweeps   */
-  int32_t pad;
+  int32_t ib_mode;           /* 0: accumulated_explicit (ib_driver_np.py:447-525);
+                                1: direct, explicit; 2: direct, implicit -- the force
+                                of every inner iteration replaces the last, times
+                                rou*ib_alpha (ib_driver_np.py:466-486)             */
+  double ib_alpha;           /* ib_mode 1, 2: force relaxation (Driver.ib_alpha)   */
 } pyib_params;
 
 /* Per-solve statistics (Driver.helm_solve finish(), ib_driver_np.py:338-377). */

@@ -29,7 +29,10 @@ def test_defaults_and_normalisation():
     ({"runtime": {"precision": "float32"}}, "precision"),
     ({"mesh": {"kind": "uniform_box", "dx": 0.3, "bounds": [[-1, 1], [-1, 1], [-1, 1]]}}, "multiples"),
     ({"time": {"inner_iterations": 1}}, "two fluid inner"),
-    ({"ib": {"force_mode": "direct"}}, "accumulated_explicit"),
+    ({"ib": {"force_mode": "replacement"}}, "force_mode must be"),
+    ({"ib": {"implicit": True}}, "explicit IB method"),
+    ({"ib": {"alpha": 0.5}}, "alpha=1.0"),
+    ({"ib": {"force_mode": "direct", "implicit": True, "alpha": 0.9}}, "alpha <= 0.7"),
     ({"case": {"kind": "oscillating_sphere"}}, "requires ib.motion.kind"),
     ({"bogus": 1}, "unknown key"),
     ({"mesh": {"kind": "nested_boxes", "cells_per_diameter": 8}}, "half_widths_d"),
@@ -43,6 +46,14 @@ def test_rejections(patch, msg):
             raw[k] = v
     with pytest.raises(CS.CaseConfigError, match=msg):
         CS.validate_config(raw)
+
+
+def test_direct_force_mode_is_accepted():
+    raw = json.loads(json.dumps(SMOKE))
+    raw["ib"].update({"force_mode": "direct", "implicit": True, "alpha": 0.5})
+    raw["time"]["inner_iterations"] = 1
+    cfg = CS.validate_config(raw)
+    assert cfg["ib"]["force_mode"] == "direct" and cfg["ib"]["implicit"] and cfg["ib"]["alpha"] == 0.5
 
 
 def test_fingerprint_ignores_output_and_steps():

@@ -23,7 +23,7 @@ def test_ctypes_structs_match_header_sizes():
     import ctypes as C
     # pyib_layout: 4 + 3*3*8*4 + 8*8 + 24*8 + 3*8 + 2*4, padded to 8
     assert C.sizeof(_lib.Layout) == 4 + 3 * 96 + 64 + 192 + 4 + 24 + 8
-    assert C.sizeof(_lib.Params) == 6 * 8 + 6 * 4 + 3 * 8 + 2 * 4
+    assert C.sizeof(_lib.Params) == 6 * 8 + 6 * 4 + 3 * 8 + 2 * 4 + 8
     assert C.sizeof(_lib.SolveStats) == 8 + 4 * 8 + 8
     assert C.sizeof(_lib.StepStats) == 16 + 16
 
