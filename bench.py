@@ -605,6 +605,128 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+PRESSURE_AXIS = 128          # cells per axis of the pressure-recovery lattice (2,097,152 cells)
+PRESSURE_CPU_AXIS = 64       # the CPU sample: the same lattice at 64^3 (262,144 cells)
+
+
+def pressure_inputs(axis):
+    """Uniform lattice graph of the offline pressure recovery (the reference's test
+    construction) with a quadratic gradient plus seeded noise."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pressure_oracle as PO
+    pos, faces, area = PO.uniform_graph(axis, 1.0 / axis)
+    rng = np.random.default_rng(17)
+    grad = PO.quadratic_gradient(pos) + 0.1 * rng.standard_normal(pos.shape)
+    return pos, faces, area, grad
+
+
+def pressure_cpu_sample():
+    """scipy CG of the reference's recover_pressure (the oracle restatement) on the
+    64^3 sample; returns (row-iterations/s, seconds, sample text)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pressure_oracle as PO
+    pos, faces, area, grad = pressure_inputs(PRESSURE_CPU_AXIS)
+    t0 = time.perf_counter()
+    _, diag = PO.recover_pressure(pos, faces, area, grad)
+    sec = time.perf_counter() - t0
+    rows = PRESSURE_CPU_AXIS ** 3 - 1
+    return rows * diag["iterations"] / sec, sec, (f"oracle (scipy cg, the reference's algorithm) recover_pressure on "
+                                                  f"{PRESSURE_CPU_AXIS}^3 cells, {diag['iterations']} iterations, "
+                                                  f"{sec:.2f} s including assembly")
+
+
+def run_pressure(args, world, rank, local):
+    """Offline pressure recovery: graph-CG row-iterations/s on a 128^3 lattice graph.
+
+    ``value``: rows x iterations / device time of the CG (events around the
+    iterations; the matrix already resident).  ``e2e``: the same work over the
+    wall time of ``recover_pressure`` (host assembly, copies, CG, gauge).  Replicas
+    for N > 1 (each rank recovers its own snapshot).
+    """
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        vals, sample = [], ""
+        for k in range(args.warmup + args.steps):
+            v, _, sample = pressure_cpu_sample()
+            if k >= args.warmup:
+                vals.append(v)
+        value = float(np.mean(vals))
+        print(json.dumps({
+            "impl": "reference", "metric": "pressure-recovery CG row-iterations/s", "value": value,
+            "unit": "row-iterations/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "pressure_recovery_128", "cpu_sample_axis": PRESSURE_CPU_AXIS},
+            "cpu_baseline": {"value": value, "unit": "row-iterations/s", "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "row-iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return 0
+    from pyib_b200 import build
+    from pyib_b200 import postprocess as PP
+    build.build_library()
+    import torch
+    torch.cuda.set_device(local)
+    dist = maybe_init_dist(world, local)
+    pos, faces, area, grad = pressure_inputs(PRESSURE_AXIS)
+    h = PP.bare_handle(local)
+    timing = (C.c_double * 5)()
+    for _ in range(args.warmup):
+        PP.recover_pressure(pos, faces, area, grad, handle=h)
+    barrier(dist)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    h.call("pyib_cg_timing", timing, 1)
+    solve_ms, e2e_s, iters, nnz = [], [], [], 0
+    for _ in range(args.steps):
+        t = {}
+        t0 = time.perf_counter()
+        _, diag = PP.recover_pressure(pos, faces, area, grad, handle=h, timing=t)
+        e2e_s.append(time.perf_counter() - t0)
+        solve_ms.append(t["solve_ms"])
+        iters.append(diag["iterations"])
+        nnz = t["nnz"]
+    clocks = sampler.stop() if sampler else None
+    h.call("pyib_cg_timing", timing, 0)
+    launches = int(timing[2])
+    rows = PRESSURE_AXIS ** 3 - 1
+    dev_s = reduce_max(dist, sum(solve_ms) / 1000.0)
+    wall = reduce_max(dist, sum(e2e_s))
+    work = float(rows) * sum(iters) * world
+    bytes_iter = 128.0 * rows + 12.0 * nnz          # algorithmic bytes of one CG iteration
+    hbm, peak_kind = peaks()
+    achieved = bytes_iter * sum(iters) / (sum(solve_ms) / 1000.0) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sec, sample = pressure_cpu_sample()
+        cpu = {"value": v, "unit": "row-iterations/s", "cores": 1, "kind": "port", "sample": sample}
+    h.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "pressure-recovery CG row-iterations/s", "value": work / dev_s, "unit": "row-iterations/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "pressure_recovery_128", "cells": rows + 1, "faces": int(len(faces)),
+                   "nnz_reduced": nnz, "cg_iterations": iters, "tolerance": 1e-10,
+                   "l2": "inputs larger than L2 (the CG streams 0.44 GB per iteration)"},
+        "e2e": {"value": work / wall, "unit": "row-iterations/s", "seconds_per_recovery": wall / args.steps,
+                "h2d_bytes_per_step": int(8 * (rows + 1) + 12 * nnz + 8 * rows),
+                "d2h_bytes_per_step": int(8 * rows)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                     "bytes_per_iteration": bytes_iter},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -633,6 +755,8 @@ def main():
                               "counterpart (the reference runs one case per process)"}), flush=True)
             return 0
         return run_batch(args, world, rank, local)
+    if args.workload == "pressure_recovery_128":
+        return run_pressure(args, world, rank, local)
     if args.compare_precision:
         return run_precision_compare(args, world, rank, local)
     if args.harmonic:

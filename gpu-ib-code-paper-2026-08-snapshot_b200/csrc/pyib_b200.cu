@@ -1003,6 +1003,88 @@ __global__ void k_dinv(long long ne, const double* __restrict__ d1, const double
 }
 
 // ---------------------------------------------------------------------------
+// Jacobi-preconditioned CG on a caller's CSR matrix (the offline pressure
+// recovery's graph Laplacian, ib_postprocess.py:49-107).  Deterministic sums.
+// ---------------------------------------------------------------------------
+struct GState {
+  double rz, rr, bb, atol, alpha, beta;
+  unsigned int counter;
+  int done, iters;
+};
+
+// The stop test of scipy.sparse.linalg.cg (atol = 0): |r| < rtol |b|, checked
+// before every iteration; once it holds every kernel below returns at once, so
+// chunks of launches may run past convergence without changing x.
+__global__ void __launch_bounds__(kThreads) k_g_init(long long n, double rtol, const double* __restrict__ b,
+                                                     const double* __restrict__ dinv, double* x, double* r,
+                                                     double* z, double* p, double* partials, GState* g) {
+  double v[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double bi = b[i], zi = dinv[i] * bi;
+    x[i] = 0.0; r[i] = bi; z[i] = zi; p[i] = zi;
+    v[0] += bi * zi;
+    v[1] += bi * bi;
+  }
+  if (grid_sum<2>(v, partials, &g->counter)) {
+    g->rz = v[0]; g->bb = v[1]; g->rr = v[1];
+    g->atol = rtol * sqrt(v[1]);
+    g->iters = 0;
+    g->done = v[1] == 0.0 || sqrt(v[1]) < g->atol;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_g_matvec(long long n, const long long* __restrict__ ptr,
+                                                       const int* __restrict__ col, const double* __restrict__ val,
+                                                       const double* __restrict__ p, double* q, const GState* g) {
+  if (g->done) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (long long k = ptr[i]; k < ptr[i + 1]; ++k) acc += val[k] * p[col[k]];
+    q[i] = acc;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_g_pq(long long n, const double* __restrict__ p,
+                                                   const double* __restrict__ q, double* partials, GState* g) {
+  if (g->done) return;
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[0] += p[i] * q[i];
+  if (grid_sum<1>(v, partials, &g->counter)) g->alpha = v[0] != 0.0 ? g->rz / v[0] : 0.0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_g_update(long long n, const double* __restrict__ p,
+                                                       const double* __restrict__ q, const double* __restrict__ dinv,
+                                                       double* x, double* r, double* z, double* partials, GState* g) {
+  if (g->done) return;
+  const double a = g->alpha;
+  double v[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    r[i] = ri;
+    const double zi = dinv[i] * ri;
+    z[i] = zi;
+    v[0] += ri * zi;
+    v[1] += ri * ri;
+  }
+  if (grid_sum<2>(v, partials, &g->counter)) {
+    g->beta = g->rz != 0.0 ? v[0] / g->rz : 0.0;
+    g->rz = v[0];
+    g->rr = v[1];
+    g->iters += 1;
+    if (sqrt(v[1]) < g->atol) g->done = 1;
+  }
+}
+
+__global__ void k_g_p(long long n, const double* __restrict__ z, double* p, const GState* g) {
+  if (g->done) return;
+  const double b = g->beta;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = z[i] + b * p[i];
+}
+
+// ---------------------------------------------------------------------------
 // generic CSR gathers (step operators)
 // ---------------------------------------------------------------------------
 __global__ void k_csr(long long nrows, const long long* __restrict__ ptr, const int* __restrict__ col,
@@ -2715,6 +2797,96 @@ int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms) {
   CK(cudaEventElapsedTime(&ms, ctx->tev0, ctx->tev1));
   if (elapsed_ms) *elapsed_ms = ms;
   return PYIB_OK;
+}
+
+int pyib_graph_pcg(pyib_ctx* ctx, int64_t n, const int64_t* ptr, const int32_t* col, const double* val,
+                   const double* rhs, double* x, double rtol, int32_t max_iterations, int32_t* iterations,
+                   double* solve_ms) {
+  if (!ctx || n <= 0 || !ptr || !col || !val || !rhs || !x || !(rtol > 0.0) || max_iterations <= 0)
+    return PYIB_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const long long nnz = ptr[n];
+  if (ptr[0] != 0 || nnz <= 0 || nnz >= (1LL << 40)) return set_err(ctx, PYIB_E_ARG, "bad CSR row pointers");
+  if (n >= (1LL << 31)) return set_err(ctx, PYIB_E_ARG, "too many rows for int32 columns");
+  // every index the device reads is checked here first
+  for (long long i = 0; i < n; ++i)
+    if (ptr[i + 1] < ptr[i]) return set_err(ctx, PYIB_E_ARG, "CSR row pointers decrease at row %lld", i);
+  for (long long k = 0; k < nnz; ++k)
+    if (col[k] < 0 || col[k] >= n) return set_err(ctx, PYIB_E_ARG, "CSR column %d out of range at %lld", col[k], k);
+  // the matrix and vectors live only for this call (offline use)
+  long long* dptr = nullptr; int* dcol = nullptr; double *dval = nullptr, *buf = nullptr, *dparts = nullptr;
+  GState* gs = nullptr;
+  auto release = [&]() {
+    cudaFree(dptr); cudaFree(dcol); cudaFree(dval); cudaFree(buf); cudaFree(dparts); cudaFree(gs);
+  };
+  int rc = [&]() -> int {
+    CK(cudaMalloc((void**)&dptr, (n + 1) * sizeof(long long)));
+    CK(cudaMalloc((void**)&dcol, nnz * sizeof(int)));
+    CK(cudaMalloc((void**)&dval, nnz * sizeof(double)));
+    CK(cudaMalloc((void**)&buf, 7 * n * sizeof(double)));
+    CK(cudaMalloc((void**)&dparts, 2 * (size_t)kPartStride * sizeof(double)));
+    CK(cudaMalloc((void**)&gs, sizeof(GState)));
+    CK(cudaMemsetAsync(gs, 0, sizeof(GState), ctx->stream));
+    CK(cudaMemcpyAsync(dptr, ptr, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dcol, col, nnz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dval, val, nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    double *b = buf, *dx = buf + n, *r = buf + 2 * n, *z = buf + 3 * n, *p = buf + 4 * n, *q = buf + 5 * n,
+           *dinv = buf + 6 * n;
+    CK(cudaMemcpyAsync(b, rhs, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    {
+      // Jacobi: 1 / diagonal, read from the host CSR
+      std::vector<double> dh(n, 0.0);
+      for (long long i = 0; i < n; ++i)
+        for (long long k = ptr[i]; k < ptr[i + 1]; ++k)
+          if (col[k] == i) dh[i] += val[k];
+      for (long long i = 0; i < n; ++i) {
+        if (!(dh[i] > 0.0)) return set_err(ctx, PYIB_E_ARG, "row %lld has no positive diagonal", i);
+        dh[i] = 1.0 / dh[i];
+      }
+      CK(cudaMemcpyAsync(dinv, dh.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    k_g_init<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, rtol, b, dinv, dx, r, z, p, dparts, gs);
+    CKL();
+    GState h{};
+    CK(cudaMemcpyAsync(&h, gs, sizeof(GState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    int launched = 0;
+    while (!h.done && launched < max_iterations) {
+      const int chunk = std::min(16, max_iterations - launched);
+      for (int c = 0; c < chunk; ++c) {
+        k_g_matvec<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, dptr, dcol, dval, p, q, gs);
+        CKL();
+        k_g_pq<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, p, q, dparts, gs);
+        CKL();
+        k_g_update<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, p, q, dinv, dx, r, z, dparts, gs);
+        CKL();
+        k_g_p<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, z, p, gs);
+        CKL();
+      }
+      launched += chunk;
+      CK(cudaMemcpyAsync(&h, gs, sizeof(GState), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (!std::isfinite(h.rr)) return set_err(ctx, PYIB_E_NONFINITE, "graph PCG: non-finite residual");
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (solve_ms) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      *solve_ms = ms;
+    }
+    const int it = h.iters;
+    if (iterations) *iterations = it;
+    if (!h.done)
+      return set_err(ctx, PYIB_E_NOCONV, "graph PCG did not converge in %d iterations (|r|/|b| = %.3e)", it,
+                     std::sqrt(h.rr / (h.bb > 0.0 ? h.bb : 1.0)));
+    return PYIB_OK;
+  }();
+  release();
+  return rc;
 }
 
 int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {

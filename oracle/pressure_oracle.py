@@ -1,0 +1,98 @@
+"""CPU oracle of the offline pressure recovery (test infrastructure only).
+
+THIS MODULE IS THE CHECKER, NOT THE PRODUCT.  Only ``tests/`` and the CPU
+leg of ``bench.py`` may import it.
+
+Restates ``recover_pressure`` of the reference (``src/pyib/solver/ib_postprocess.py:49-107``)
+with SciPy, as the reference itself computes it: the signed face-cell incidence B
+over internal faces, weights ``A / |x2 - x1|``, jumps ``(g1 + g2)/2 . (x2 - x1)``,
+the Laplacian ``B^T W B`` reduced by pinning cell 0 (rows and columns 1..n-1),
+``scipy.sparse.linalg.cg`` with the Jacobi preconditioner, ``rtol = tolerance``,
+``atol = 0``, ``maxiter = max(2000, 10 n)``, then the boundary-adjacent mean
+removed (``ib_postprocess.py:99-102``).
+
+Parity pin: ``tests/test_pressure_oracle.py`` checks this restatement against
+``tests/golden/pressure_n2_mesh.npz``, made by running the reference's own
+function (``tests/golden/make_pressure_golden.py``), and against the
+reference's quadratic known-answer case (``tests/test_ib_postprocess.py:76-84``).
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.sparse import coo_matrix, diags
+from scipy.sparse.csgraph import connected_components
+from scipy.sparse.linalg import cg
+
+
+def recover_pressure(cell_positions, face_cells, face_area, gradient, *, tolerance=1e-10):
+    """Returns (pressure, diagnostics) with the reference's keys plus ``iterations``."""
+    pos = np.asarray(cell_positions, dtype=np.float64)
+    grad = np.asarray(gradient, dtype=np.float64)
+    pairs = np.asarray(face_cells)
+    area = np.asarray(face_area, dtype=np.float64)
+    n = len(pos)
+    inner = pairs[:, 1] >= 0
+    a, b = pairs[inner, 0], pairs[inner, 1]
+    d = pos[b] - pos[a]
+    w = area[inner] / np.linalg.norm(d, axis=1)
+    m = len(a)
+    inc = coo_matrix((np.r_[-np.ones(m), np.ones(m)], (np.r_[np.arange(m), np.arange(m)], np.r_[a, b])),
+                     shape=(m, n)).tocsr()
+    lap = (inc.T @ diags(w) @ inc).tocsr()
+    if connected_components(lap, directed=False, return_labels=False) != 1:
+        raise ValueError("pressure graph is disconnected; a unique gauge is unavailable")
+    jump = 0.5 * np.sum((grad[a] + grad[b]) * d, axis=1)
+    rhs = np.asarray(inc.T @ (w * jump))
+    red = lap[1:, 1:]
+    count = [0]
+
+    def tick(_):
+        count[0] += 1
+
+    p = np.zeros(n)
+    p[1:], status = cg(red, rhs[1:], M=diags(1.0 / red.diagonal()), rtol=tolerance, atol=0.0,
+                       maxiter=max(2000, 10 * n), callback=tick)
+    if status != 0:
+        raise RuntimeError(f"pressure graph solve failed to converge (status {status})")
+    edge = np.unique(pairs[~inner, 0])
+    if not len(edge):
+        edge = np.arange(n)
+    p -= p[edge].mean()
+    mis = inc @ p - jump
+    return p, {
+        "gauge": "mean boundary-adjacent cells = 0" if np.any(~inner) else "mean cells = 0",
+        "gradient_projection_weighted_rms": float(np.sqrt(np.sum(w * mis**2) / w.sum())),
+        "iterations": count[0],
+    }
+
+
+def uniform_graph(count, spacing):
+    """Cell centres, face pairs (boundary faces with -1) and areas of a count^3 block,
+    built as in the reference's test helper (``tests/test_ib_postprocess.py:18-33``)."""
+    ids = np.arange(count**3).reshape((count,) * 3)
+    axes = (np.arange(count) - 0.5 * (count - 1)) * spacing
+    pos = np.stack(np.meshgrid(axes, axes, axes, indexing="ij"), axis=-1).reshape(-1, 3)
+    faces = []
+    for axis in range(3):
+        lo, hi = [slice(None)] * 3, [slice(None)] * 3
+        lo[axis], hi[axis] = slice(None, -1), slice(1, None)
+        faces.append(np.column_stack((ids[tuple(lo)].ravel(), ids[tuple(hi)].ravel())))
+        for side in (0, -1):
+            sel = [slice(None)] * 3
+            sel[axis] = side
+            cells = ids[tuple(sel)].ravel()
+            faces.append(np.column_stack((cells, np.full(len(cells), -1))))
+    faces = np.concatenate(faces)
+    return pos, faces, np.full(len(faces), spacing**2)
+
+
+def quadratic(points):
+    """The manufactured pressure of the reference's test (``tests/test_ib_postprocess.py:44-46``)."""
+    x, y, z = np.asarray(points).T
+    return 1.3 + 0.2 * x - 0.5 * y + 0.7 * z + 0.4 * x * x - 0.2 * y * y + 0.3 * z * z + 0.1 * x * y
+
+
+def quadratic_gradient(points):
+    """Its gradient (``tests/test_ib_postprocess.py:49-51``)."""
+    x, y, z = np.asarray(points).T
+    return np.column_stack((0.2 + 0.8 * x + 0.1 * y, -0.5 - 0.4 * y + 0.1 * x, 0.7 + 0.6 * z))

@@ -1,0 +1,101 @@
+"""Offline pressure recovery with the graph CG on the device, against the oracle
+and the reference's outputs (tests/golden/pressure_golden.npz)."""
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+
+import pressure_oracle as PO
+import parity_util as PU
+from pyib_b200 import _lib
+from pyib_b200 import postprocess as PP
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(PU.GOLDEN / "pressure_golden.npz")
+
+
+def n2_inputs():
+    g = PU.golden("n2_fixed")
+    n = int(g["mesh_ncell"])
+    return g["geo_cpos"][:n], g["mesh_F2C"], g["geo_Af"], GOLD["n2_gradient"]
+
+
+def test_nested_mesh_graph_matches_reference():
+    """Same stop test as scipy's cg: the pressure agrees to rounding of the
+    iterates (1e-9 of its range; the CG stops at |r| < 1e-10 |b|)."""
+    args = n2_inputs()
+    p, diag = PP.recover_pressure(*args)
+    want = GOLD["n2_pressure"]
+    ref = json.loads(str(GOLD["n2_diag"]))
+    assert np.max(np.abs(p - want)) <= 1e-9 * np.max(np.abs(want))
+    assert diag["gauge"] == ref["gauge"]
+    assert diag["gradient_projection_weighted_rms"] == pytest.approx(ref["gradient_projection_weighted_rms"],
+                                                                     rel=1e-8)
+    _, odiag = PO.recover_pressure(*args)
+    assert abs(diag["iterations"] - odiag["iterations"]) <= 2
+    # deterministic: a second call gives the same bits
+    p2, _ = PP.recover_pressure(*args)
+    np.testing.assert_array_equal(p, p2)
+
+
+def test_quadratic_known_answer_9():
+    """The reference's 9^3 case and bounds (tests/test_ib_postprocess.py:76-84)."""
+    pos, faces, area = PO.uniform_graph(9, 0.25)
+    p, diag = PP.recover_pressure(pos, faces, area, PO.quadratic_gradient(pos))
+    expected = PO.quadratic(pos)
+    boundary = np.unique(faces[faces[:, 1] < 0, 0])
+    expected -= expected[boundary].mean()
+    np.testing.assert_allclose(p, expected, atol=3e-9, rtol=1e-8)
+    assert abs(p[boundary].mean()) < 1e-14
+    assert diag["gradient_projection_weighted_rms"] < 1e-9
+    np.testing.assert_allclose(p, GOLD["q9_pressure"], rtol=0, atol=1e-12)
+
+
+def test_noisy_48_matches_oracle():
+    pos, faces, area = PO.uniform_graph(48, 1.0 / 48)
+    rng = np.random.default_rng(3)
+    grad = PO.quadratic_gradient(pos) + 0.1 * rng.standard_normal(pos.shape)
+    p, diag = PP.recover_pressure(pos, faces, area, grad)
+    q, odiag = PO.recover_pressure(pos, faces, area, grad)
+    assert np.max(np.abs(p - q)) <= 1e-9 * np.max(np.abs(q))
+    assert abs(diag["iterations"] - odiag["iterations"]) <= 2
+    assert diag["gradient_projection_weighted_rms"] == pytest.approx(odiag["gradient_projection_weighted_rms"],
+                                                                     rel=1e-8)
+
+
+def test_quadratic_known_answer_128_cubed():
+    """2.1 M cells: the projection of an exact quadratic gradient is the quadratic
+    (second-order jumps are exact on a uniform lattice), to the CG tolerance."""
+    c = 128
+    pos, faces, area = PO.uniform_graph(c, 1.0 / c)
+    p, diag = PP.recover_pressure(pos, faces, area, PO.quadratic_gradient(pos))
+    expected = PO.quadratic(pos)
+    boundary = np.unique(faces[faces[:, 1] < 0, 0])
+    expected -= expected[boundary].mean()
+    assert np.max(np.abs(p - expected)) <= 1e-9
+    assert diag["gradient_projection_weighted_rms"] < 1e-9
+    assert 0 < diag["iterations"] < 10 * c ** 3
+
+
+def test_solver_handle_is_reused_and_errors_are_reported():
+    args = n2_inputs()
+    h = PP.bare_handle(0)
+    try:
+        p, _ = PP.recover_pressure(*args, handle=h)
+        np.testing.assert_array_equal(p, PP.recover_pressure(*args)[0])
+        ptr, col, val, rhs, _ = PP.assemble(*args)
+        with pytest.raises(_lib.B200Error) as exc:
+            PP.graph_pcg(h, ptr, col, val, rhs, 1e-10, 3)
+        assert exc.value.code == _lib.E_NOCONV
+        bad = col.copy()
+        bad[5] = len(rhs)                   # rejected on the host before any launch
+        with pytest.raises(_lib.B200Error) as exc:
+            PP.graph_pcg(h, ptr, bad, val, rhs, 1e-10, 100)
+        assert exc.value.code == _lib.E_ARG
+        # the context stays usable after both errors
+        x, it = PP.graph_pcg(h, ptr, col, val, rhs, 1e-10, 5000)
+        assert it > 0 and np.all(np.isfinite(x))
+    finally:
+        h.close()
