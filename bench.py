@@ -640,7 +640,8 @@ def run_pressure(args, world, rank, local):
 
     ``value``: rows x iterations / device time of the CG (events around the
     iterations; the matrix already resident).  ``e2e``: the same work over the
-    wall time of ``recover_pressure`` (host assembly, copies, CG, gauge).  Replicas
+    wall time of ``recover_pressure`` (shape checks, copies of the inputs, device
+    assembly and checks, CG, gauge, copy of the pressure).  Replicas
     for N > 1 (each rank recovers its own snapshot).
     """
     import _pyib_b200_import
@@ -679,15 +680,16 @@ def run_pressure(args, world, rank, local):
     if sampler:
         sampler.start()
     h.call("pyib_cg_timing", timing, 1)
-    solve_ms, e2e_s, iters, nnz = [], [], [], 0
+    solve_ms, dev_ms, e2e_s, iters, nnz, sweeps = [], [], [], [], 0, 0
     for _ in range(args.steps):
         t = {}
         t0 = time.perf_counter()
         _, diag = PP.recover_pressure(pos, faces, area, grad, handle=h, timing=t)
         e2e_s.append(time.perf_counter() - t0)
         solve_ms.append(t["solve_ms"])
+        dev_ms.append(t["device_ms"])
         iters.append(diag["iterations"])
-        nnz = t["nnz"]
+        nnz, sweeps = t["nnz"], t["sweeps"]
     clocks = sampler.stop() if sampler else None
     h.call("pyib_cg_timing", timing, 0)
     launches = int(timing[2])
@@ -695,7 +697,11 @@ def run_pressure(args, world, rank, local):
     dev_s = reduce_max(dist, sum(solve_ms) / 1000.0)
     wall = reduce_max(dist, sum(e2e_s))
     work = float(rows) * sum(iters) * world
-    bytes_iter = 128.0 * rows + 12.0 * nnz          # algorithmic bytes of one CG iteration
+    # algorithmic bytes of one CG iteration: the matvec + p.q kernel reads ptr and p once
+    # per row and col + val per nonzero and writes q (24 B per row + 12 B per nonzero);
+    # the update reads p, q, dinv, x, r and writes x, r, z (64 B); the direction reads
+    # z, p and writes p (24 B)
+    bytes_iter = 112.0 * (rows + 1) + 12.0 * nnz
     hbm, peak_kind = peaks()
     achieved = bytes_iter * sum(iters) / (sum(solve_ms) / 1000.0) / 1e9
     cpu = None
@@ -713,11 +719,12 @@ def run_pressure(args, world, rank, local):
         "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "pressure_recovery_128", "cells": rows + 1, "faces": int(len(faces)),
-                   "nnz_reduced": nnz, "cg_iterations": iters, "tolerance": 1e-10,
-                   "l2": "inputs larger than L2 (the CG streams 0.44 GB per iteration)"},
+                   "csr_nonzeros": nnz, "cg_iterations": iters, "tolerance": 1e-10,
+                   "device_ms_per_recovery": sum(dev_ms) / len(dev_ms), "connectivity_sweeps": sweeps,
+                   "l2": "inputs larger than L2 (the CG streams 0.42 GB per iteration)"},
         "e2e": {"value": work / wall, "unit": "row-iterations/s", "seconds_per_recovery": wall / args.steps,
-                "h2d_bytes_per_step": int(8 * (rows + 1) + 12 * nnz + 8 * rows),
-                "d2h_bytes_per_step": int(8 * rows)},
+                "h2d_bytes_per_step": int(48 * (rows + 1) + 24 * len(faces)),
+                "d2h_bytes_per_step": int(8 * (rows + 1))},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
                      "bytes_per_iteration": bytes_iter},

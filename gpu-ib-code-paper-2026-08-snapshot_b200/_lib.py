@@ -42,6 +42,7 @@ EXPORTS = [
     "pyib_operator", "pyib_calc_vel", "pyib_conv_diff", "pyib_helm_solve", "pyib_step",
     "pyib_ib_stencil", "pyib_ib_interp", "pyib_ib_spread", "pyib_loads", "pyib_diagnostics",
     "pyib_cg_timing", "pyib_event", "pyib_bench_matvec", "pyib_spread_noalloc", "pyib_ib_interp_dx", "pyib_graph_pcg",
+    "pyib_recover_pressure",
 ]
 
 
@@ -138,6 +139,7 @@ def load():
         "pyib_ib_interp_dx": [vp, C.POINTER(C.c_double)],
         "pyib_graph_pcg": [vp, C.c_int64, vp, vp, vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
                            C.POINTER(C.c_double)],
+        "pyib_recover_pressure": [vp, C.c_int64, vp, C.c_int64, vp, vp, vp, C.c_double, C.c_int32, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -120,6 +120,10 @@ struct pyib_ctx {
          *dL = nullptr, *ibw = nullptr;
   int *ibcell = nullptr, *ibbase = nullptr;
   double* ibjac = nullptr;        // 9 per marker: d u_L / d x_marker (pyib_ib_interp_dx)
+  void* ws = nullptr;             // grow-only workspace of the offline graph calls
+  size_t ws_bytes = 0;
+  void* ws_tmp = nullptr;         // grow-only CUB temporary storage of those calls
+  size_t ws_tmp_bytes = 0;
   int imp_iters = 0;              // CG iterations of the last implicit IB solve
   int *sort_keys_in = nullptr, *sort_keys_out = nullptr, *sort_vals_in = nullptr,
       *sort_vals_out = nullptr;
@@ -1033,23 +1037,21 @@ __global__ void __launch_bounds__(kThreads) k_g_init(long long n, double rtol, c
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_g_matvec(long long n, const long long* __restrict__ ptr,
-                                                       const int* __restrict__ col, const double* __restrict__ val,
-                                                       const double* __restrict__ p, double* q, const GState* g) {
+// q = A p and the p.q sum for alpha in one pass (one row per thread); the
+// thread-to-row map and the order of the sums are those of a separate p.q kernel
+// on the same grid.
+__global__ void __launch_bounds__(kThreads) k_g_mvpq(long long n, const long long* __restrict__ ptr,
+                                                     const int* __restrict__ col, const double* __restrict__ val,
+                                                     const double* __restrict__ p, double* __restrict__ q,
+                                                     double* partials, GState* g) {
   if (g->done) return;
+  double v[1] = {0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     double acc = 0.0;
     for (long long k = ptr[i]; k < ptr[i + 1]; ++k) acc += val[k] * p[col[k]];
     q[i] = acc;
+    v[0] += p[i] * acc;
   }
-}
-
-__global__ void __launch_bounds__(kThreads) k_g_pq(long long n, const double* __restrict__ p,
-                                                   const double* __restrict__ q, double* partials, GState* g) {
-  if (g->done) return;
-  double v[1] = {0.0};
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    v[0] += p[i] * q[i];
   if (grid_sum<1>(v, partials, &g->counter)) g->alpha = v[0] != 0.0 ? g->rz / v[0] : 0.0;
 }
 
@@ -1082,6 +1084,170 @@ __global__ void k_g_p(long long n, const double* __restrict__ z, double* p, cons
   const double b = g->beta;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     p[i] = z[i] + b * p[i];
+}
+
+
+// ---------------------------------------------------------------------------
+// Offline pressure recovery on the device (ib_postprocess.py:49-107): input
+// checks, the face weights and jumps, the Laplacian in CSR (cell 0 pinned: its
+// row is empty and rhs[0] = dinv[0] = 0, so p[0] stays 0 and its column adds
+// exact zeros), a reachability sweep for the connectivity check, the gauge and
+// the projection residual.  Sums are in fixed orders: per-row sums follow the
+// sorted (neighbour, face) keys, grid sums follow the block order.
+// ---------------------------------------------------------------------------
+enum : unsigned { kPrPos = 1u, kPrGrad = 2u, kPrIds = 4u, kPrAreaNf = 8u, kPrAreaNeg = 16u, kPrDist = 32u };
+
+struct PrState {
+  unsigned int err;
+  unsigned int counter;
+  unsigned long long reached;
+};
+
+__global__ void k_pr_cells(long long n3, const double* __restrict__ pos, const double* __restrict__ grad,
+                           PrState* st) {
+  unsigned int e = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
+    if (!isfinite(pos[i])) e |= kPrPos;
+    if (!isfinite(grad[i])) e |= kPrGrad;
+  }
+  if (e) atomicOr(&st->err, e);
+}
+
+// per face: ids checked before any use; internal faces get w = A/|d| and the jump
+// 0.5 (g1 + g2).d, summed in the reference's component order
+__global__ void k_pr_faces(long long nf, long long n, const long long* __restrict__ pairs,
+                           const double* __restrict__ area, const double* __restrict__ pos,
+                           const double* __restrict__ grad, unsigned int* deg, double* w_f, double* jump_f,
+                           unsigned char* bflag, PrState* st) {
+  unsigned int e = 0;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+    const long long a = pairs[2 * f], b = pairs[2 * f + 1];
+    w_f[f] = 0.0;
+    jump_f[f] = 0.0;
+    if (a < 0 || a >= n || b < -1 || b >= n) { e |= kPrIds; continue; }
+    const double ar = area[f];
+    if (!isfinite(ar)) e |= kPrAreaNf;
+    else if (!(ar > 0.0)) e |= kPrAreaNeg;
+    if (b < 0) { bflag[a] = 1; continue; }
+    const double dx = pos[3 * b] - pos[3 * a], dy = pos[3 * b + 1] - pos[3 * a + 1], dz = pos[3 * b + 2] - pos[3 * a + 2];
+    const double dist = sqrt((dx * dx + dy * dy) + dz * dz);
+    if (!(dist > 0.0)) { e |= kPrDist; continue; }
+    const double s0 = (grad[3 * a] + grad[3 * b]) * dx, s1 = (grad[3 * a + 1] + grad[3 * b + 1]) * dy,
+                 s2 = (grad[3 * a + 2] + grad[3 * b + 2]) * dz;
+    const double w = ar / dist;
+    w_f[f] = w;
+    jump_f[f] = 0.5 * ((s0 + s1) + s2);
+    if (w > 0.0) {                 // the same test as k_pr_fill: one key per count
+      atomicAdd(&deg[a], 1u);
+      atomicAdd(&deg[b], 1u);
+    }
+  }
+  if (e) atomicOr(&st->err, e);
+}
+
+// key lengths per row (row 0 pinned: none); klen has n + 1 entries, the last 0
+__global__ void k_pr_klen(long long n, const unsigned int* __restrict__ deg, int* klen) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c <= n; c += (long long)gridDim.x * blockDim.x)
+    klen[c] = (c == 0 || c == n) ? 0 : (int)deg[c];
+}
+
+// key = (neighbour << 32) | (face << 1) | side, side 1 when the row's cell is the face's second cell
+__global__ void k_pr_fill(long long nf, const long long* __restrict__ pairs, const double* __restrict__ w_f,
+                          int* kcur, unsigned long long* keys) {
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+    const long long a = pairs[2 * f], b = pairs[2 * f + 1];
+    if (b < 0 || !(w_f[f] > 0.0)) continue;
+    const unsigned long long lo = (unsigned long long)f << 1;
+    if (a != 0) keys[atomicAdd(&kcur[a], 1)] = ((unsigned long long)b << 32) | lo;
+    if (b != 0) keys[atomicAdd(&kcur[b], 1)] = ((unsigned long long)a << 32) | lo | 1ull;
+  }
+}
+
+// one row per thread: diagonal first, then the neighbours in key order
+__global__ void k_pr_rows(long long n, const int* __restrict__ kptr, const unsigned long long* __restrict__ keys,
+                          const double* __restrict__ w_f, const double* __restrict__ jump_f, long long* ptr, int* col,
+                          double* val, double* rhs, double* dinv) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (c == n - 1) ptr[n] = (long long)kptr[n] + (n - 1);
+    if (c == 0) {
+      ptr[0] = 0;
+      rhs[0] = 0.0;
+      dinv[0] = 0.0;
+      continue;
+    }
+    const long long base = (long long)kptr[c] + (c - 1);
+    ptr[c] = base;
+    double diag = 0.0, sum = 0.0;
+    long long o = base + 1;
+    for (int k = kptr[c]; k < kptr[c + 1]; ++k, ++o) {
+      const unsigned long long key = keys[k];
+      const long long f = (long long)((key & 0xffffffffull) >> 1);
+      const double w = w_f[f], wj = w * jump_f[f];
+      diag += w;
+      sum += (key & 1ull) ? wj : -wj;
+      col[o] = (int)(key >> 32);
+      val[o] = -w;
+    }
+    col[base] = (int)c;
+    val[base] = diag;
+    rhs[c] = sum;
+    dinv[c] = diag > 0.0 ? 1.0 / diag : 0.0;
+  }
+}
+
+// cells reachable from cell 0: a cell joins when a neighbour in its row has
+// joined (monotone, so concurrent sweeps only speed it up)
+__global__ void __launch_bounds__(kThreads) k_pr_reach(long long n, const long long* __restrict__ ptr,
+                                                       const int* __restrict__ col, volatile unsigned char* vis,
+                                                       PrState* st) {
+  __shared__ unsigned int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  unsigned int mine = 0;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    if (vis[c]) continue;
+    for (long long k = ptr[c] + 1; k < ptr[c + 1]; ++k)
+      if (vis[col[k]]) {
+        vis[c] = 1;
+        ++mine;
+        break;
+      }
+  }
+  if (mine) atomicAdd(&cnt, mine);
+  __syncthreads();
+  if (threadIdx.x == 0 && cnt) atomicAdd(&st->reached, (unsigned long long)cnt);
+}
+
+__global__ void __launch_bounds__(kThreads) k_pr_gauge(long long n, const double* __restrict__ x,
+                                                       const unsigned char* __restrict__ bflag, double* partials,
+                                                       unsigned int* counter, double* out) {
+  double v[3] = {0.0, 0.0, 0.0};
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const double xc = x[c];
+    if (bflag[c]) { v[0] += xc; v[1] += 1.0; }
+    v[2] += xc;
+  }
+  if (grid_sum<3>(v, partials, counter)) { out[0] = v[0]; out[1] = v[1]; out[2] = v[2]; }
+}
+
+__global__ void k_pr_shift(long long n, double* x, double mean) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    x[c] -= mean;
+}
+
+__global__ void __launch_bounds__(kThreads) k_pr_mismatch(long long nf, const long long* __restrict__ pairs,
+                                                          const double* __restrict__ x, const double* __restrict__ w_f,
+                                                          const double* __restrict__ jump_f, double* partials,
+                                                          unsigned int* counter, double* out) {
+  double v[2] = {0.0, 0.0};
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+    const long long b = pairs[2 * f + 1];
+    if (b < 0) continue;
+    const double w = w_f[f], m = (x[b] - x[pairs[2 * f]]) - jump_f[f];
+    v[0] += w * (m * m);
+    v[1] += w;
+  }
+  if (grid_sum<2>(v, partials, counter)) { out[0] = v[0]; out[1] = v[1]; }
 }
 
 // ---------------------------------------------------------------------------
@@ -2336,6 +2502,63 @@ int bench_matvec_t(pyib_ctx* ctx, int reps, const T* in, T* out, T* vcm, T* vq, 
   return PYIB_OK;
 }
 
+// Carves 256-byte aligned pieces out of one buffer; with base == nullptr it only
+// adds up the size.
+struct Carve {
+  char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+// grows *buf to at least bytes (the stream is drained first: the old buffer may be in use)
+static int grow(pyib_ctx* ctx, void** buf, size_t* have, size_t bytes) {
+  if (bytes <= *have && *buf) return PYIB_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *have = 0;
+  CK(cudaMalloc(buf, bytes < 256 ? 256 : bytes));
+  *have = bytes < 256 ? 256 : bytes;
+  return PYIB_OK;
+}
+
+// Jacobi PCG from zero on a device CSR (three kernels per iteration).  Chunks of
+// 16 iterations between reads of the state; kernels after convergence return at once.
+static int graph_cg(pyib_ctx* ctx, long long n, const long long* ptr, const int* col, const double* val,
+                    const double* b, const double* dinv, double* x, double* r, double* z, double* p, double* q,
+                    double rtol, int max_iterations, double* parts, GState* gs, GState& h) {
+  cudaStream_t st = ctx->stream;
+  CK(cudaEventRecord(ctx->ev0, st));
+  k_g_init<<<grid_for(n), kThreads, 0, st>>>(n, rtol, b, dinv, x, r, z, p, parts, gs);
+  CKL();
+  CK(cudaMemcpyAsync(&h, gs, sizeof(GState), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  int launched = 0;
+  while (!h.done && launched < max_iterations) {
+    const int chunk = std::min(16, max_iterations - launched);
+    for (int c = 0; c < chunk; ++c) {
+      k_g_mvpq<<<grid_for(n), kThreads, 0, st>>>(n, ptr, col, val, p, q, parts, gs);
+      CKL();
+      k_g_update<<<grid_for(n), kThreads, 0, st>>>(n, p, q, dinv, x, r, z, parts, gs);
+      CKL();
+      k_g_p<<<grid_for(n), kThreads, 0, st>>>(n, z, p, gs);
+      CKL();
+    }
+    launched += chunk;
+    CK(cudaMemcpyAsync(&h, gs, sizeof(GState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!std::isfinite(h.rr)) return set_err(ctx, PYIB_E_NONFINITE, "graph PCG: non-finite residual");
+  }
+  CK(cudaEventRecord(ctx->ev1, st));
+  return PYIB_OK;
+}
+
 extern "C" {
 
 int pyib_version(char* buf, size_t n) {
@@ -2460,7 +2683,7 @@ int pyib_destroy(pyib_ctx* ctx) {
                   ctx->ibcell, ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
                   ctx->sort_vals_out, ctx->sort_tmp, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
                   ctx->vcm32, ctx->vq32, ctx->prec32, ctx->pa_val32, ctx->pv_val32,
-                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->ibjac};
+                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->ibjac, ctx->ws, ctx->ws_tmp};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
@@ -2813,19 +3036,23 @@ int pyib_graph_pcg(pyib_ctx* ctx, int64_t n, const int64_t* ptr, const int32_t* 
     if (ptr[i + 1] < ptr[i]) return set_err(ctx, PYIB_E_ARG, "CSR row pointers decrease at row %lld", i);
   for (long long k = 0; k < nnz; ++k)
     if (col[k] < 0 || col[k] >= n) return set_err(ctx, PYIB_E_ARG, "CSR column %d out of range at %lld", col[k], k);
-  // the matrix and vectors live only for this call (offline use)
-  long long* dptr = nullptr; int* dcol = nullptr; double *dval = nullptr, *buf = nullptr, *dparts = nullptr;
-  GState* gs = nullptr;
-  auto release = [&]() {
-    cudaFree(dptr); cudaFree(dcol); cudaFree(dval); cudaFree(buf); cudaFree(dparts); cudaFree(gs);
+  // the matrix and vectors live in the context's grow-only workspace
+  long long* dptr; int* dcol; double *dval, *buf, *dparts;
+  GState* gs;
+  auto carve = [&](Carve& c) {
+    dptr = c.take<long long>(n + 1);
+    dcol = c.take<int>(nnz);
+    dval = c.take<double>(nnz);
+    buf = c.take<double>(7 * n);
+    dparts = c.take<double>(2 * (size_t)kPartStride);
+    gs = c.take<GState>(1);
   };
+  Carve size{nullptr};
+  carve(size);
+  RET(grow(ctx, &ctx->ws, &ctx->ws_bytes, size.off));
+  Carve real{(char*)ctx->ws};
+  carve(real);
   int rc = [&]() -> int {
-    CK(cudaMalloc((void**)&dptr, (n + 1) * sizeof(long long)));
-    CK(cudaMalloc((void**)&dcol, nnz * sizeof(int)));
-    CK(cudaMalloc((void**)&dval, nnz * sizeof(double)));
-    CK(cudaMalloc((void**)&buf, 7 * n * sizeof(double)));
-    CK(cudaMalloc((void**)&dparts, 2 * (size_t)kPartStride * sizeof(double)));
-    CK(cudaMalloc((void**)&gs, sizeof(GState)));
     CK(cudaMemsetAsync(gs, 0, sizeof(GState), ctx->stream));
     CK(cudaMemcpyAsync(dptr, ptr, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(dcol, col, nnz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
@@ -2846,31 +3073,8 @@ int pyib_graph_pcg(pyib_ctx* ctx, int64_t n, const int64_t* ptr, const int32_t* 
       CK(cudaMemcpyAsync(dinv, dh.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
     }
-    CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    k_g_init<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, rtol, b, dinv, dx, r, z, p, dparts, gs);
-    CKL();
     GState h{};
-    CK(cudaMemcpyAsync(&h, gs, sizeof(GState), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    int launched = 0;
-    while (!h.done && launched < max_iterations) {
-      const int chunk = std::min(16, max_iterations - launched);
-      for (int c = 0; c < chunk; ++c) {
-        k_g_matvec<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, dptr, dcol, dval, p, q, gs);
-        CKL();
-        k_g_pq<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, p, q, dparts, gs);
-        CKL();
-        k_g_update<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, p, q, dinv, dx, r, z, dparts, gs);
-        CKL();
-        k_g_p<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, z, p, gs);
-        CKL();
-      }
-      launched += chunk;
-      CK(cudaMemcpyAsync(&h, gs, sizeof(GState), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (!std::isfinite(h.rr)) return set_err(ctx, PYIB_E_NONFINITE, "graph PCG: non-finite residual");
-    }
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    RET(graph_cg(ctx, n, dptr, dcol, dval, b, dinv, dx, r, z, p, q, rtol, max_iterations, dparts, gs, h));
     CK(cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (solve_ms) {
@@ -2885,7 +3089,171 @@ int pyib_graph_pcg(pyib_ctx* ctx, int64_t n, const int64_t* ptr, const int32_t* 
                      std::sqrt(h.rr / (h.bb > 0.0 ? h.bb : 1.0)));
     return PYIB_OK;
   }();
-  release();
+  return rc;
+}
+
+int pyib_recover_pressure(pyib_ctx* ctx, int64_t ncell, const double* positions, int64_t nface,
+                          const int64_t* face_cells, const double* face_area, const double* gradient, double rtol,
+                          int32_t max_iterations, double* pressure, double* info) {
+  if (!ctx || !positions || !face_cells || !face_area || !gradient || !pressure || !(rtol > 0.0) ||
+      max_iterations <= 0)
+    return PYIB_E_ARG;
+  if (ncell < 2) return set_err(ctx, PYIB_E_ARG, "pressure recovery needs at least two 3D cells");
+  if (ncell >= (1LL << 31) || nface >= (1LL << 30) || nface < 0)
+    return set_err(ctx, PYIB_E_ARG, "pressure graph too large (%lld cells, %lld faces)", (long long)ncell,
+                   (long long)nface);
+  if (nface == 0) return set_err(ctx, PYIB_E_ARG, "pressure graph has no valid internal faces");
+  CK(cudaSetDevice(ctx->device));
+  const long long n = ncell, nf = nface;
+  cudaStream_t st = ctx->stream;
+  // every buffer lives in the context's grow-only workspace, sized for the
+  // largest key count (two per face)
+  double *dpos, *dgrad, *darea, *w_f, *jump_f, *val, *buf, *dparts, *dout;
+  long long *dpairs, *ptr;
+  unsigned int* deg;
+  int *klen, *kptr, *kcur, *col;
+  unsigned long long *keys, *keys_sorted;
+  unsigned char *bflag, *vis;
+  PrState* pst;
+  GState* gs;
+  auto carve = [&](Carve& c) {
+    dpos = c.take<double>(3 * n);
+    dgrad = c.take<double>(3 * n);
+    darea = c.take<double>(nf);
+    dpairs = c.take<long long>(2 * nf);
+    w_f = c.take<double>(nf);
+    jump_f = c.take<double>(nf);
+    deg = c.take<unsigned int>(n);
+    klen = c.take<int>(n + 1);
+    kptr = c.take<int>(n + 1);
+    kcur = c.take<int>(n + 1);
+    bflag = c.take<unsigned char>(n);
+    vis = c.take<unsigned char>(n);
+    pst = c.take<PrState>(1);
+    gs = c.take<GState>(1);
+    dparts = c.take<double>(3 * (size_t)kPartStride);
+    dout = c.take<double>(4);
+    buf = c.take<double>(7 * n);
+    keys = c.take<unsigned long long>(2 * nf);
+    keys_sorted = c.take<unsigned long long>(2 * nf);
+    ptr = c.take<long long>(n + 1);
+    col = c.take<int>(2 * nf + n);
+    val = c.take<double>(2 * nf + n);
+  };
+  Carve size{nullptr};
+  carve(size);
+  RET(grow(ctx, &ctx->ws, &ctx->ws_bytes, size.off));
+  Carve real{(char*)ctx->ws};
+  carve(real);
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  int rc = [&]() -> int {
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, st));
+    CK(cudaMemcpyAsync(dpos, positions, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dgrad, gradient, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(darea, face_area, nf * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dpairs, face_cells, 2 * nf * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(deg, 0, n * sizeof(unsigned int), st));
+    CK(cudaMemsetAsync(bflag, 0, n, st));
+    CK(cudaMemsetAsync(pst, 0, sizeof(PrState), st));
+    CK(cudaMemsetAsync(gs, 0, sizeof(GState), st));
+    k_pr_cells<<<grid_for(3 * n), kThreads, 0, st>>>(3 * n, dpos, dgrad, pst);
+    CKL();
+    k_pr_faces<<<grid_for(nf), kThreads, 0, st>>>(nf, n, dpairs, darea, dpos, dgrad, deg, w_f, jump_f, bflag, pst);
+    CKL();
+    k_pr_klen<<<grid_for(n + 1), kThreads, 0, st>>>(n, deg, klen);
+    CKL();
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, klen, kptr, (int)(n + 1), st));
+    RET(grow(ctx, &ctx->ws_tmp, &ctx->ws_tmp_bytes, tb));
+    CK(cub::DeviceScan::ExclusiveSum(ctx->ws_tmp, tb, klen, kptr, (int)(n + 1), st));
+    PrState hs{};
+    int nkeys = 0;
+    unsigned int deg0 = 0;
+    CK(cudaMemcpyAsync(&hs, pst, sizeof(PrState), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&nkeys, kptr + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&deg0, deg, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // the reference's checks, in its order (ib_postprocess.py:58-79, 88-89)
+    if (hs.err & kPrPos) return set_err(ctx, PYIB_E_ARG, "cell_positions contains non-finite values");
+    if (hs.err & kPrGrad) return set_err(ctx, PYIB_E_ARG, "gradient contains non-finite values");
+    if (hs.err & kPrIds) return set_err(ctx, PYIB_E_ARG, "face_cells contains invalid cell ids");
+    if (hs.err & kPrAreaNf) return set_err(ctx, PYIB_E_ARG, "face_area contains non-finite values");
+    if (hs.err & kPrAreaNeg) return set_err(ctx, PYIB_E_ARG, "face areas must be positive");
+    if ((hs.err & kPrDist) || (long long)nkeys + deg0 == 0)
+      return set_err(ctx, PYIB_E_ARG, "pressure graph has no valid internal faces");
+    // CSR rows: keys sorted within each row
+    const long long nnz = (long long)nkeys + (n - 1);
+    CK(cudaMemcpyAsync(kcur, kptr, (n + 1) * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    k_pr_fill<<<grid_for(nf), kThreads, 0, st>>>(nf, dpairs, w_f, kcur, keys);
+    CKL();
+    if (nkeys > 0) {
+      size_t sb = 0;
+      CK(cub::DeviceSegmentedSort::SortKeys(nullptr, sb, keys, keys_sorted, nkeys, (int)n, kptr, kptr + 1, st));
+      RET(grow(ctx, &ctx->ws_tmp, &ctx->ws_tmp_bytes, sb));
+      CK(cub::DeviceSegmentedSort::SortKeys(ctx->ws_tmp, sb, keys, keys_sorted, nkeys, (int)n, kptr, kptr + 1, st));
+    }
+    double *b = buf, *dx = buf + n, *r = buf + 2 * n, *z = buf + 3 * n, *p = buf + 4 * n, *q = buf + 5 * n,
+           *dinv = buf + 6 * n;
+    k_pr_rows<<<grid_for(n), kThreads, 0, st>>>(n, kptr, keys_sorted, w_f, jump_f, ptr, col, val, b, dinv);
+    CKL();
+    // connectivity: sweeps until a chunk reaches no new cell (at most n productive sweeps)
+    CK(cudaMemsetAsync(vis, 0, n, st));
+    CK(cudaMemsetAsync(vis, 1, 1, st));
+    unsigned long long seen = 0;
+    long long sweeps = 0;
+    for (;;) {
+      for (int c = 0; c < 8; ++c) {
+        k_pr_reach<<<grid_for(n), kThreads, 0, st>>>(n, ptr, col, vis, pst);
+        CKL();
+      }
+      sweeps += 8;
+      CK(cudaMemcpyAsync(&hs, pst, sizeof(PrState), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (hs.reached == seen || hs.reached >= (unsigned long long)(n - 1) || sweeps > n + 8) break;
+      seen = hs.reached;
+    }
+    if (hs.reached != (unsigned long long)(n - 1))
+      return set_err(ctx, PYIB_E_ARG, "pressure graph is disconnected; a unique gauge is unavailable");
+    // the CG (scipy's stop test), from zero
+    GState h{};
+    RET(graph_cg(ctx, n, ptr, col, val, b, dinv, dx, r, z, p, q, rtol, max_iterations, dparts, gs, h));
+    if (!h.done)
+      return set_err(ctx, PYIB_E_NOCONV, "pressure graph solve failed to converge (status %d)", max_iterations);
+    // gauge: the mean over the cells with a boundary face (every cell if none)
+    double g3[3];
+    k_pr_gauge<<<grid_for(n), kThreads, 0, st>>>(n, dx, bflag, dparts, &gs->counter, dout);
+    CKL();
+    CK(cudaMemcpyAsync(g3, dout, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const bool boundary = g3[1] > 0.0;
+    const double mean = boundary ? g3[0] / g3[1] : g3[2] / (double)n;
+    k_pr_shift<<<grid_for(n), kThreads, 0, st>>>(n, dx, mean);
+    CKL();
+    double m2[2];
+    k_pr_mismatch<<<grid_for(nf), kThreads, 0, st>>>(nf, dpairs, dx, w_f, jump_f, dparts, &gs->counter, dout);
+    CKL();
+    CK(cudaMemcpyAsync(m2, dout, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(pressure, dx, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(t1, st));
+    CK(cudaStreamSynchronize(st));
+    if (info) {
+      float solve = 0.f, total = 0.f;
+      CK(cudaEventElapsedTime(&solve, ctx->ev0, ctx->ev1));
+      CK(cudaEventElapsedTime(&total, t0, t1));
+      info[0] = std::sqrt(m2[0] / m2[1]);
+      info[1] = (double)h.iters;
+      info[2] = boundary ? 1.0 : 0.0;
+      info[3] = solve;
+      info[4] = total;
+      info[5] = (double)sweeps;
+      info[6] = (double)nnz;
+    }
+    return PYIB_OK;
+  }();
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
   return rc;
 }
 

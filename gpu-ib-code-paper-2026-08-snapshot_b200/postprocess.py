@@ -10,10 +10,13 @@ the reference's ``recover_pressure`` (``ib_postprocess.py:49-107``):
   (scipy's ``cg`` with ``atol = 0``) and at most ``max(2000, 10 n)`` iterations;
 * the mean over the boundary-adjacent cells (every cell if none) is removed.
 
-The Laplacian is assembled on the host in O(faces) (sort by (row, column));
-the CG, which dominates at a million cells, runs in ``pyib_graph_pcg``
-(deterministic sums, one row per thread).  There is no CPU solve: the call
-fails if the library is missing.  The reference's band repair
+Everything after the shape checks runs on the device in one call
+(``pyib_recover_pressure``): the value checks, the face weights and jumps, the
+Laplacian in CSR (rows sorted by neighbour and face), the connectivity check,
+the CG and the gauge, all with sums in fixed orders.  ``assemble`` builds the
+same reduced system on the host for callers of the generic CSR solver
+``graph_pcg`` (``pyib_graph_pcg``).  There is no CPU solve: the calls fail if
+the library is missing.  The reference's band repair
 (``ib_postprocess.py:213-250``, an lsqr on the few cells next to the body) is
 not part of this module.
 """
@@ -88,7 +91,7 @@ def graph_pcg(handle, ptr, col, val, rhs, tolerance, max_iterations, timing=None
 
 
 def assemble(cell_positions, face_cells, face_area, gradient):
-    """Validated inputs to the reduced system (``ib_postprocess.py:58-89``).
+    """The reduced system on the host, for ``graph_pcg`` (``ib_postprocess.py:58-89``).
 
     Returns ``(ptr, col, val, rhs, graph)``: the CSR of the Laplacian with cell 0
     pinned (rows and columns 1..n-1), its right-hand side, and a dict with the
@@ -132,45 +135,76 @@ def assemble(cell_positions, face_cells, face_area, gradient):
     return rptr, seg_col[keep] - 1, seg_val[keep], rhs[1:], faces
 
 
+def _validate_host(cell_positions, face_cells, face_area, gradient):
+    """The reference's checks in its order, on the host: run only when an input's
+    shape or type already fails, so that the first failing check is the one reported."""
+    positions = _finite("cell_positions", cell_positions)
+    count = len(positions)
+    if positions.shape != (count, 3) or count < 2:
+        raise ValueError("pressure recovery needs at least two 3D cells")
+    _finite("gradient", gradient, positions.shape)
+    pairs = np.asarray(face_cells)
+    if pairs.ndim != 2 or pairs.shape[1] != 2 or pairs.dtype.kind not in "iu":
+        raise ValueError("face_cells must be an integer (number_of_faces, 2) array")
+    if np.any(pairs[:, 0] < 0) or np.any(pairs >= count) or np.any(pairs[:, 1] < -1):
+        raise ValueError("face_cells contains invalid cell ids")
+    _finite("face_area", face_area, (len(pairs),))
+
+
 def recover_pressure(cell_positions, face_cells, face_area, gradient, *, tolerance=1e-10,
                      handle=None, device=0, timing=None):
     """Cell pressure whose face jumps best match the cell pressure gradients.
 
     Same arguments, result and errors as the reference (ValueError for invalid or
-    disconnected input, RuntimeError when the solve does not converge).  ``handle``
-    reuses an existing context (a solver's ``h``); otherwise one is made on ``device``.
-    The returned diagnostics add ``iterations``; ``timing`` (a dict) receives
-    ``solve_ms`` (device time of the CG) and ``nnz``.
+    disconnected input, RuntimeError when the solve does not converge).  Shapes and
+    types are checked here; the value checks, the assembly, the connectivity check,
+    the CG, the gauge and the residual run on the device (``pyib_recover_pressure``).
+    ``handle`` reuses an existing context (a solver's ``h``); otherwise one is made
+    on ``device``.  The diagnostics add ``iterations``; ``timing`` (a dict) receives
+    ``solve_ms`` (the CG), ``device_ms`` (the whole call on the device, copies
+    included), ``sweeps`` (connectivity) and ``nnz``.
     """
-    ptr, col, val, rhs, fc = assemble(cell_positions, face_cells, face_area, gradient)
-    count = fc["count"]
-    if timing is not None:
-        timing["nnz"] = int(len(col))
+    pos = np.asarray(cell_positions, dtype=np.float64)
+    grad = np.asarray(gradient, dtype=np.float64)
+    pairs = np.asarray(face_cells)
+    area = np.asarray(face_area, dtype=np.float64)
+    if not (pos.ndim == 2 and pos.shape[1] == 3 and len(pos) >= 2 and grad.shape == pos.shape
+            and pairs.ndim == 2 and pairs.shape[1] == 2 and pairs.dtype.kind in "iu"
+            and area.shape == (len(pairs),)):
+        _validate_host(pos, pairs, area, grad)
+        raise ValueError("invalid pressure-recovery inputs")
+    pos = np.ascontiguousarray(pos)
+    grad = np.ascontiguousarray(grad)
+    area = np.ascontiguousarray(area)
+    pairs64 = np.ascontiguousarray(pairs, dtype=np.int64)
+    if pairs.dtype.kind == "u" and len(pairs) and pairs.max() >= len(pos):
+        _validate_host(pos, pairs, area, grad)     # ids that do not fit int64
+    count = len(pos)
     max_it = max(2000, 10 * count)
+    out = np.empty(count)
+    info = np.zeros(7)
     own = handle is None
     h = bare_handle(device) if own else handle
     try:
-        try:
-            sol, iters = graph_pcg(h, ptr, col, val, rhs, tolerance, max_it, timing)
-        except _lib.B200Error as exc:
-            if exc.code == _lib.E_NOCONV:
-                raise RuntimeError(f"pressure graph solve failed to converge (status {max_it})") from exc
-            raise
+        rc = h.lib.pyib_recover_pressure(
+            h.ptr, C.c_int64(count), pos.ctypes.data_as(C.c_void_p), C.c_int64(len(pairs64)),
+            pairs64.ctypes.data_as(C.c_void_p), area.ctypes.data_as(C.c_void_p), grad.ctypes.data_as(C.c_void_p),
+            C.c_double(tolerance), C.c_int32(int(max_it)), out.ctypes.data_as(C.c_void_p),
+            info.ctypes.data_as(C.c_void_p))
+        if rc == _lib.E_ARG:
+            raise ValueError(h.error())
+        if rc == _lib.E_NOCONV:
+            raise RuntimeError(h.error())
+        if rc != _lib.OK:
+            raise _lib.B200Error(rc, f"pyib_recover_pressure: {h.error()}")
     finally:
         if own:
             h.close()
-    pressure = np.zeros(count)
-    pressure[1:] = sol
-    pairs, internal = fc["pairs"], fc["internal"]
-    gauge_cells = np.unique(pairs[~internal, 0])
-    if not len(gauge_cells):
-        gauge_cells = np.arange(count)
-    pressure -= np.mean(pressure[gauge_cells])
-    weights = fc["weights"]
-    mismatch = (pressure[fc["second"]] - pressure[fc["first"]]) - fc["jumps"]
+    if timing is not None:
+        timing.update(solve_ms=float(info[3]), device_ms=float(info[4]), sweeps=int(info[5]), nnz=int(info[6]))
     diagnostics = {
-        "gauge": "mean boundary-adjacent cells = 0" if np.any(~internal) else "mean cells = 0",
-        "gradient_projection_weighted_rms": float(np.sqrt(np.sum(weights * mismatch**2) / weights.sum())),
-        "iterations": iters,
+        "gauge": "mean boundary-adjacent cells = 0" if info[2] else "mean cells = 0",
+        "gradient_projection_weighted_rms": float(info[0]),
+        "iterations": int(info[1]),
     }
-    return pressure, diagnostics
+    return out, diagnostics

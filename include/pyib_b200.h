@@ -226,6 +226,22 @@ int pyib_graph_pcg(pyib_ctx* ctx, int64_t n, const int64_t* ptr, const int32_t* 
 /* ClosedSphereLoadCorrection.evaluate + fluid force/moment integrals
  * (ib_interior.py:216-239, 291-296).  out[0:3] force_fluid, [3:6] moment_fluid,
  * [6:9] linear momentum, [9:12] angular momentum, [12] indicator volume. */
+/* Offline pressure recovery, all of it on the device (ib_postprocess.py:49-107,
+ * recover_pressure): input checks with the reference's messages (PYIB_E_ARG),
+ * the face weights A/|x2-x1| and jumps 0.5 (g1+g2).(x2-x1), the Laplacian with
+ * cell 0 pinned, the connectivity check, Jacobi-preconditioned CG from zero with
+ * the stop |r| < rtol |b| (scipy's cg, atol = 0; PYIB_E_NOCONV after
+ * max_iterations), the boundary-adjacent zero-mean gauge and the weighted
+ * projection residual.  Host arrays: positions and gradient ncell x 3, face_cells
+ * nface x 2 (second cell -1 on boundary faces), face_area nface; pressure
+ * receives ncell doubles.  info (nullable, 7 doubles): weighted residual rms,
+ * iterations, 1 if the gauge used boundary cells, CG device ms, whole-call device
+ * ms (copies included), connectivity sweeps, CSR nonzeros.  All sums are in fixed
+ * orders, so repeated calls give the same bits. */
+int pyib_recover_pressure(pyib_ctx* ctx, int64_t ncell, const double* positions, int64_t nface,
+                          const int64_t* face_cells, const double* face_area, const double* gradient, double rtol,
+                          int32_t max_iterations, double* pressure, double* info);
+
 int pyib_loads(pyib_ctx* ctx, const double* centre, double radius, double width,
                double density, int32_t fixed_centre, const double* centre0, double* out);
 

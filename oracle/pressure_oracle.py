@@ -24,6 +24,36 @@ from scipy.sparse.csgraph import connected_components
 from scipy.sparse.linalg import cg
 
 
+def recover_pressure_checked(cell_positions, face_cells, face_area, gradient, *, tolerance=1e-10):
+    """The reference's input checks in its order (``ib_postprocess.py:58-79``), then the solve."""
+    def finite(name, values, shape=None):
+        values = np.asarray(values, dtype=np.float64)
+        if shape is not None and values.shape != shape:
+            raise ValueError(f"{name} must have shape {shape}, got {values.shape}")
+        if not np.isfinite(values).all():
+            raise ValueError(f"{name} contains non-finite values")
+        return values
+
+    pos = finite("cell_positions", cell_positions)
+    n = len(pos)
+    if pos.shape != (n, 3) or n < 2:
+        raise ValueError("pressure recovery needs at least two 3D cells")
+    grad = finite("gradient", gradient, pos.shape)
+    pairs = np.asarray(face_cells)
+    if pairs.ndim != 2 or pairs.shape[1] != 2 or pairs.dtype.kind not in "iu":
+        raise ValueError("face_cells must be an integer (number_of_faces, 2) array")
+    if np.any(pairs[:, 0] < 0) or np.any(pairs >= n) or np.any(pairs[:, 1] < -1):
+        raise ValueError("face_cells contains invalid cell ids")
+    area = finite("face_area", face_area, (len(pairs),))
+    if np.any(area <= 0):
+        raise ValueError("face areas must be positive")
+    inner = pairs[:, 1] >= 0
+    dist = np.linalg.norm(pos[pairs[inner, 1]] - pos[pairs[inner, 0]], axis=1)
+    if not len(dist) or np.any(dist <= 0):
+        raise ValueError("pressure graph has no valid internal faces")
+    return recover_pressure(pos, pairs, area, grad, tolerance=tolerance)
+
+
 def recover_pressure(cell_positions, face_cells, face_area, gradient, *, tolerance=1e-10):
     """Returns (pressure, diagnostics) with the reference's keys plus ``iterations``."""
     pos = np.asarray(cell_positions, dtype=np.float64)

@@ -99,3 +99,55 @@ def test_solver_handle_is_reused_and_errors_are_reported():
         assert it > 0 and np.all(np.isfinite(x))
     finally:
         h.close()
+
+
+@pytest.mark.parametrize("case, message", [
+    (dict(faces=np.array([[0, 5]])), "face_cells contains invalid cell ids"),
+    (dict(faces=np.array([[0, 1], [1, -2]]), area=np.ones(2)), "face_cells contains invalid cell ids"),
+    (dict(area=np.array([-1.0])), "face areas must be positive"),
+    (dict(area=np.array([np.nan])), "face_area contains non-finite values"),
+    (dict(grad=np.full((2, 3), np.nan)), "gradient contains non-finite values"),
+    (dict(pos=np.array([[0.0, 0, 0], [np.inf, 0, 0]]), area=np.array([-1.0])),
+     "cell_positions contains non-finite values"),
+    (dict(faces=np.array([[0, -1]])), "pressure graph has no valid internal faces"),
+    (dict(pos=np.zeros((2, 3))), "pressure graph has no valid internal faces"),
+])
+def test_value_errors_found_on_the_device(case, message):
+    """Value checks run on the device and report the reference's first failing check."""
+    kw = dict(pos=np.array([[0.0, 0, 0], [1.0, 0, 0]]), faces=np.array([[0, 1]]), area=np.ones(1),
+              grad=np.zeros((2, 3)))
+    kw.update(case)
+    with pytest.raises(ValueError, match=message):
+        PP.recover_pressure(kw["pos"], kw["faces"], kw["area"], kw["grad"])
+    with pytest.raises(ValueError, match=message):
+        PO.recover_pressure_checked(kw["pos"], kw["faces"], kw["area"], kw["grad"])
+
+
+def test_disconnected_graph_is_rejected():
+    """The reference's own case (tests/test_ib_postprocess.py:112-116), and a
+    two-block lattice with no face between the blocks."""
+    with pytest.raises(ValueError, match="disconnected"):
+        PP.recover_pressure(np.array([[0., 0., 0.], [1., 0., 0.], [3., 0., 0.]]), np.array([[0, 1], [2, -1]]),
+                            np.ones(2), np.zeros((3, 3)))
+    pos, faces, area = PO.uniform_graph(8, 0.25)
+    keep = ~((faces[:, 1] >= 0) & ((pos[faces[:, 0], 0] < 0) != (pos[np.maximum(faces[:, 1], 0), 0] < 0)))
+    with pytest.raises(ValueError, match="disconnected"):
+        PP.recover_pressure(pos, faces[keep], area[keep], np.zeros_like(pos))
+
+
+def test_device_assembly_matches_host_assembly():
+    """The device's CSR (sorted rows, diagonal first) and the host's sorted-key CSR
+    solve the same system: the pressures agree to the CG tolerance."""
+    args = n2_inputs()
+    p, diag = PP.recover_pressure(*args)
+    h = PP.bare_handle(0)
+    try:
+        ptr, col, val, rhs, _ = PP.assemble(*args)
+        x, it = PP.graph_pcg(h, ptr, col, val, rhs, 1e-10, 32400)
+    finally:
+        h.close()
+    q = np.r_[0.0, x]
+    boundary = np.unique(args[1][args[1][:, 1] < 0, 0])
+    q -= q[boundary].mean()
+    assert np.max(np.abs(p - q)) <= 1e-9 * np.max(np.abs(q))
+    assert abs(it - diag["iterations"]) <= 2
