@@ -145,6 +145,8 @@ struct pyib_ctx {
   long long cg_iters = 0;
   long long launches = 0;        // kernels launched by this context
   bool tuned = false;            // matvec tile depths chosen by timing
+  Meta meta32{};                 // the float32 matvec's copy of meta, with its own tile depths
+  bool tuned32 = false;
   double tune_ms = 0.0;          // best matvec time seen by the tuner
 };
 
@@ -737,7 +739,7 @@ __device__ __forceinline__ double prec_of(const Meta& m, const unsigned int* __r
 
 // r -= alpha w on unmasked edges; eta' = sum (r*prec)*r; the last block applies the
 // stopping test (every `check` iterations, or at cg_max) and sets `stop`.
-__global__ void __launch_bounds__(kThreads) k_cg_update(Meta m, long long ne, double* r,
+__global__ void __launch_bounds__(kThreads, 8) k_cg_update(Meta m, long long ne, double* r,
                                                         const double* __restrict__ w,
                                                         const unsigned int* __restrict__ pbits,
                                                         const double* __restrict__ prec,
@@ -745,8 +747,27 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(Meta m, long long ne, do
   if (st->done) return;
   const double alpha = st->alpha;
   double v[1] = {0.0};
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x) {
+  // two elements of the thread's grid-stride sequence per pass, loads first (more
+  // bytes in flight); each element is computed and summed in the original order
+  const long long S = (long long)gridDim.x * blockDim.x;
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; e + S < ne; e += 2 * S) {
+    double pr[2], rv[2], wv[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      pr[u] = prec_of(m, pbits, prec, e + u * S);
+      rv[u] = r[e + u * S];
+      wv[u] = w[e + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      if (pr[u] != 0.0) {
+        const double re = rv[u] - alpha * wv[u];
+        r[e + u * S] = re;
+        v[0] += (re * pr[u]) * re;
+      }
+  }
+  for (; e < ne; e += S) {
     const double pr = prec_of(m, pbits, prec, e);
     if (pr != 0.0) {
       const double re = r[e] - alpha * w[e];
@@ -904,14 +925,25 @@ __global__ void __launch_bounds__(kThreads) k_cg_update32(long long ne, float* d
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_cg_p32(long long ne, const float* __restrict__ r32,
+__global__ void __launch_bounds__(kThreads, 8) k_cg_p32(long long ne, const float* __restrict__ r32,
                                                      const float* __restrict__ dinv, float* p32,
                                                      const CGState* st) {
   if (st->done) return;
   const float beta = (float)st->beta;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x)
-    p32[e] = r32[e] * dinv[e] + beta * p32[e];
+  const long long S = (long long)gridDim.x * blockDim.x;
+  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; e + 3 * S < ne; e += 4 * S) {
+    float rv[4], dv[4], pv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      rv[u] = r32[e + u * S];
+      dv[u] = dinv[e + u * S];
+      pv[u] = p32[e + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) p32[e + u * S] = rv[u] * dv[u] + beta * pv[u];
+  }
+  for (; e < ne; e += S) p32[e] = r32[e] * dinv[e] + beta * p32[e];
 }
 
 // Reliable update of the float32 CG: r32 = float(r64) (the float64 residual after
@@ -1791,7 +1823,7 @@ int op_convdiff(pyib_ctx* ctx, int mode, double c1, double c2, double dt, const 
 template <typename T>
 int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* pdot, int alpd,
                     int do_dot, const T* pa_val, const T* pv_val, const T* pr_val) {
-  const Meta& m = ctx->meta;
+  const Meta& m = sizeof(T) == 4 ? ctx->meta32 : ctx->meta;
   const long long nc = ctx->lay.ncell;
   const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
   k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, pa_val, ctx->nA,
@@ -1873,6 +1905,59 @@ int tune_matvec(pyib_ctx* ctx) {
   ctx->tune_ms = best / 3.0;
   ctx->tuned = true;
   ctx->cg_graph_check = -1;
+  ctx->mix_graph_check = -1;
+  CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PYIB_OK;
+}
+
+// The same search for the float32 matvec of the mixed solver: its kernels wait on
+// load latency differently, so they get their own depths (meta32).  The dot's
+// partials are indexed by plane, not by chunk, so the depths do not change results.
+int tune_matvec32(pyib_ctx* ctx) {
+  if (ctx->tuned32) return PYIB_OK;
+  CGState h{};
+  CK(cudaMemcpyAsync(&h, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CGState t = h;
+  t.rou = 1.0;
+  t.kfac = 1e-3;
+  t.done = 0;
+  t.counter = 0u;
+  CK(cudaMemcpyAsync(ctx->st, &t, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  const long long ne = ctx->lay.nedge;
+  CK(cudaMemsetAsync(ctx->p32, 0, ne * sizeof(float), ctx->stream));
+  const int depths[5] = {1, 2, 4, 8, 16};
+  const Meta base = ctx->meta;
+  int bestA = base.kz, bestR = base.kzR;
+  double best = 1e30;
+  for (int a = 0; a < 5; ++a) {
+    for (int b = 0; b < 5; ++b) {
+      Meta m2 = base;
+      set_grids(m2, depths[a], depths[b]);
+      if ((long long)m2.gxR * m2.gyR * m2.gzR > kPartStride) continue;
+      ctx->meta32 = m2;
+      auto once = [&]() {
+        return launch_matvec_t<float>(ctx, ctx->p32, ctx->w32, ctx->vcm32, ctx->vq32, ctx->p32, 1, 0,
+                                      ctx->pa_val32, ctx->pv_val32, ctx->pr_val32);
+      };
+      RET(once());
+      CK(cudaEventRecord(ctx->ev0, ctx->stream));
+      for (int q = 0; q < 3; ++q) RET(once());
+      CK(cudaEventRecord(ctx->ev1, ctx->stream));
+      CK(cudaEventSynchronize(ctx->ev1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (ms < best) {
+        best = ms;
+        bestA = depths[a];
+        bestR = depths[b];
+      }
+    }
+  }
+  ctx->meta32 = base;
+  set_grids(ctx->meta32, bestA, bestR);
+  ctx->tuned32 = true;
   ctx->mix_graph_check = -1;
   CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -2149,6 +2234,7 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
   RET(tune_matvec(ctx));
   RET(ensure_mixed(ctx));
+  RET(tune_matvec32(ctx));
   RET(build_diag(ctx));
   const double kfac = 0.5 * dt * ctx->prm.visc;
   if (ctx->diag_for_kfac != kfac || ctx->diag_for_rou != ctx->prm.rou) {
@@ -2470,7 +2556,7 @@ int bench_matvec_t(pyib_ctx* ctx, int reps, const T* in, T* out, T* vcm, T* vq, 
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ms_per[0] = ms / reps;
   // each kernel alone, same inputs (after a full matvec, so every intermediate is current)
-  const Meta& m = ctx->meta;
+  const Meta& m = sizeof(T) == 4 ? ctx->meta32 : ctx->meta;
   const long long nc = ctx->lay.ncell;
   const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
   for (int kern = 0; kern < 6; ++kern) {
@@ -2545,7 +2631,8 @@ static int graph_cg(pyib_ctx* ctx, long long n, const long long* ptr, const int*
     for (int c = 0; c < chunk; ++c) {
       k_g_mvpq<<<grid_for(n), kThreads, 0, st>>>(n, ptr, col, val, p, q, parts, gs);
       CKL();
-      k_g_update<<<grid_for(n), kThreads, 0, st>>>(n, p, q, dinv, x, r, z, parts, gs);
+      // 40 registers: 6 resident blocks per SM, so one wave of 148 x 6 blocks
+      k_g_update<<<std::min(grid_for(n), 148 * 6), kThreads, 0, st>>>(n, p, q, dinv, x, r, z, parts, gs);
       CKL();
       k_g_p<<<grid_for(n), kThreads, 0, st>>>(n, z, p, gs);
       CKL();
@@ -2733,6 +2820,7 @@ int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes) {
   ctx->diag_ready = false;
   ctx->diag_for_kfac = -1.0;
   ctx->tuned = false;
+  ctx->tuned32 = false;
   return PYIB_OK;
 }
 
@@ -2743,6 +2831,7 @@ int pyib_finalize(pyib_ctx* ctx, const int64_t* counts, int32_t ncounts) {
   ctx->nR = counts[2];
   ctx->meta.ri_up = (ncounts >= 4 && counts[3] != 0) ? 0 : 1;
   set_grids(ctx->meta, ctx->meta.kz, ctx->meta.kzR);
+  ctx->tuned32 = false;
   if ((long long)ctx->meta.gxR * ctx->meta.gyR * ctx->meta.gzR + patch_grid(ctx->nR) > kPartStride ||
       (long long)ctx->meta.nplanes + patch_grid(ctx->nR) > kPartStride)
     return set_err(ctx, PYIB_E_ARG, "too many reduction slots for this layout");
@@ -3266,6 +3355,7 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
   if (ctx->prm.precision == 1) {
     // the float32 matvec of the mixed solver, on a float32 copy of WORK_E
     RET(ensure_mixed(ctx));
+    RET(tune_matvec32(ctx));
     const long long ne = ctx->lay.nedge;
     k_d2f<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->work_e, ctx->p32);
     CKL();

@@ -214,8 +214,8 @@ int pyib_ib_interp_dx(pyib_ctx* ctx, double* jac);
  * preconditioned CG from x = 0 on a caller's symmetric positive definite CSR matrix
  * (n rows; ptr[n+1], col, val on the host), stopping when |b - A x| <= rtol |b| (the
  * test of scipy.sparse.linalg.cg with atol = 0), checked every 10 iterations.  The
- * matrix and vectors are copied to the device for the call (indices are checked
- * on the host first); x (n doubles, host) receives the solution, *iterations the
+ * matrix and vectors are copied into the context's grow-only workspace (indices
+ * are checked on the host first); x (n doubles, host) receives the solution, *iterations the
  * iterations run, *solve_ms (nullable) the device time from the first kernel to
  * the last (CUDA events).  Not converged: PYIB_E_NOCONV, x holding the last iterate. */
 int pyib_graph_pcg(pyib_ctx* ctx, int64_t n, const int64_t* ptr, const int32_t* col, const double* val,
