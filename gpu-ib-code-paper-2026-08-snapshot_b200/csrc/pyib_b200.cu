@@ -600,12 +600,29 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
 // entries), so the cost is one dependent gather chain per row, overlapped
 // across all rows.
 // ---------------------------------------------------------------------------
+// The row is read in chunks of 8 entries: the chunk's columns and values are
+// loaded first, then its gathers, then the products are added in entry order,
+// so the sum is the sequential one and only the loads overlap.
 template <typename T>
 __device__ __forceinline__ T csr_row(const long long* __restrict__ ptr, const int* __restrict__ col,
                                      const T* __restrict__ val, const T* __restrict__ src, long long r) {
   const long long q0 = ptr[r], q1 = ptr[r + 1];
   T acc = 0;
-  for (long long q = q0; q < q1; ++q) acc += val[q] * src[col[q]];
+  for (long long q = q0; q < q1; q += 8) {
+    int cc[8];
+    T vv[8], xs[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const bool ok = q + u < q1;
+      cc[u] = ok ? col[q + u] : 0;
+      vv[u] = ok ? val[q + u] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) xs[u] = (q + u < q1) ? src[cc[u]] : (T)0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (q + u < q1) acc += vv[u] * xs[u];
+  }
   return acc;
 }
 
@@ -636,12 +653,30 @@ __global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __
   const int c = ids[r];
   const long long q0 = ptr[r], q1 = ptr[r + 1];
   T a0 = 0, a1 = 0, a2 = 0;
-  for (long long q = q0; q < q1; ++q) {
-    const T vv = val[q];
-    const int cc = col[q];
-    a0 += vv * v[cc];
-    a1 += vv * v[nc + cc];
-    a2 += vv * v[2 * nc + cc];
+  // chunks of 4 entries, loads first, products added in entry order (as csr_row)
+  for (long long q = q0; q < q1; q += 4) {
+    int cc[4];
+    T vv[4], x0[4], x1[4], x2[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool ok = q + u < q1;
+      cc[u] = ok ? col[q + u] : 0;
+      vv[u] = ok ? val[q + u] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool ok = q + u < q1;
+      x0[u] = ok ? v[cc[u]] : (T)0;
+      x1[u] = ok ? v[nc + cc[u]] : (T)0;
+      x2[u] = ok ? v[2 * nc + cc[u]] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q + u < q1) {
+        a0 += vv[u] * x0[u];
+        a1 += vv[u] * x1[u];
+        a2 += vv[u] * x2[u];
+      }
   }
   const T rou = (T)st->rou, kf = (T)st->kfac;
   vq[c] = rou * v[c] - kf * a0;
@@ -1079,8 +1114,7 @@ __global__ void __launch_bounds__(kThreads) k_g_mvpq(long long n, const long lon
   if (g->done) return;
   double v[1] = {0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (long long k = ptr[i]; k < ptr[i + 1]; ++k) acc += val[k] * p[col[k]];
+    const double acc = csr_row<double>(ptr, col, val, p, i);
     q[i] = acc;
     v[0] += p[i] * acc;
   }
