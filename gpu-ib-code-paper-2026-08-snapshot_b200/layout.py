@@ -160,8 +160,43 @@ class NestedLayout:
         return st
 
     # ---- per-entity tables (lazy) -----------------------------------------
+    def _state3(self, L, dims, off):
+        """cell_state of the level-L cells (i, j, k) - off for every index triple of a
+        box of ``dims``, as a (dims[2], dims[1], dims[0]) array (x fastest when
+        flattened): in-box and in-hole tests factor per axis."""
+        lv = self.levels[L]
+        idx = [np.arange(dims[t]) - off[t] for t in range(3)]
+        inb = [(idx[t] >= 0) & (idx[t] < lv.n[t]) for t in range(3)]
+        st = np.where(inb[2][:, None, None] & inb[1][None, :, None] & inb[0][None, None, :], ACTIVE, OUT)
+        if lv.hole_lo is not None:
+            inh = [(idx[t] >= lv.hole_lo[t]) & (idx[t] < lv.hole_lo[t] + lv.hole_n[t]) for t in range(3)]
+            st = np.where(inh[2][:, None, None] & inh[1][None, :, None] & inh[0][None, None, :], HOLE, st)
+        return st
+
+    @staticmethod
+    def _flat3(dims, base, off, step):
+        """base + flat(step, (i, j, k) - off) for every index triple of a box of ``dims``
+        (``step`` the dims of the numbered grid), as a 3D array like ``_state3``."""
+        i = np.arange(dims[0], dtype=np.int64) - off[0]
+        j = np.arange(dims[1], dtype=np.int64) - off[1]
+        k = np.arange(dims[2], dtype=np.int64) - off[2]
+        return base + (k[:, None, None] * step[1] + j[None, :, None]) * step[0] + i[None, None, :]
+
+    @staticmethod
+    def _coords3(dims, lo, h, shift, out):
+        """out[...] = lo + h (ijk + shift) for every index triple of a box (out: (N, 3))."""
+        o = out.reshape(dims[2], dims[1], dims[0], 3)
+        o[..., 0] = (lo[0] + h * (np.arange(dims[0]) + shift[0]))[None, None, :]
+        o[..., 1] = (lo[1] + h * (np.arange(dims[1]) + shift[1]))[None, :, None]
+        o[..., 2] = (lo[2] + h * (np.arange(dims[2]) + shift[2]))[:, None, None]
+
     def build(self):
-        """Existence masks, face cells, face-edge links and geometry (dense ids)."""
+        """Existence masks, face cells, face-edge links and geometry (dense ids).
+
+        Every entity of one level and axis has a contiguous range of dense ids in
+        x-fastest order, so each table is filled by slices of 3D arrays built from
+        per-axis 1D tests.
+        """
         NC, NF, NE = self.NC, self.NF, self.NE
         self.cell_active = np.zeros(NC, dtype=bool)
         self.cell_h = np.zeros(NC)
@@ -181,69 +216,77 @@ class NestedLayout:
         self.face_level = np.zeros(NF, dtype=np.int8)
         self.cell_level = np.zeros(NC, dtype=np.int8)
         lk_f, lk_e, lk_s, lk_x = [], [], [], []          # face-edge links (x: extra link)
+        zero = np.zeros(3, dtype=np.int64)
         for lv in self.levels:
             L, hL = lv.L, lv.h
-            cg = _grid(lv.n)
-            cid = self.cell_id(L, cg)
-            self.cell_active[cid] = self.cell_state(L, cg) == ACTIVE
-            self.cell_h[cid] = hL
-            self.cell_level[cid] = L
-            self.cpos[cid] = lv.lo + hL * (cg + 0.5)
+            cb = self.cell_base[L]
+            ncl = int(np.prod(lv.n))
+            cs = slice(cb, cb + ncl)
+            self.cell_active[cs] = (self._state3(L, lv.n, zero) == ACTIVE).ravel()
+            self.cell_h[cs] = hL
+            self.cell_level[cs] = L
+            self._coords3(lv.n, lv.lo, hL, (0.5, 0.5, 0.5), self.cpos[cs])
             for a in range(3):
                 # faces of axis a
-                fg = _grid(lv.face_dims(a))
-                fid = self.face_id(L, a, fg)
-                slo = self.cell_state(L, fg - _E[a])
-                shi = self.cell_state(L, fg)
+                fd = lv.face_dims(a)
+                fb = self.face_base[L][a]
+                fs = slice(fb, fb + int(np.prod(fd)))
+                slo = self._state3(L, fd, _E[a])
+                shi = self._state3(L, fd, zero)
                 ex = ((slo == ACTIVE) & (shi == ACTIVE)) | ((slo == ACTIVE) & (shi == OUT)) \
                     | ((slo == OUT) & (shi == ACTIVE))
-                self.face_exists[fid] = ex
-                self.face_axis[fid] = a
-                self.face_h[fid] = hL
-                self.face_level[fid] = L
-                self.fpos[fid] = lv.lo + hL * (fg + 0.5 * (1 - _E[a]))
-                lo_c = np.where(slo == ACTIVE, self.cell_id(L, fg - _E[a]), -1)
-                hi_c = np.where(shi == ACTIVE, self.cell_id(L, fg), -1)
+                self.face_exists[fs] = ex.ravel()
+                self.face_axis[fs] = a
+                self.face_h[fs] = hL
+                self.face_level[fs] = L
+                self._coords3(fd, lv.lo, hL, 0.5 * (1 - _E[a]), self.fpos[fs])
+                lo_c = np.where(slo == ACTIVE, self._flat3(fd, cb, _E[a], lv.n), -1)
+                hi_c = np.where(shi == ACTIVE, self._flat3(fd, cb, zero, lv.n), -1)
                 if L + 1 < self.N:                        # interface faces: coarse neighbour
                     up = self.levels[L + 1]
-                    m = ex & (slo == OUT)
-                    cc = up.hole_lo + np.floor_divide(fg[m] - _E[a], 2)
-                    lo_c[m] = self.cell_id(L + 1, cc)
-                    m = ex & (shi == OUT)
-                    cc = up.hole_lo + np.floor_divide(fg[m], 2)
-                    hi_c[m] = self.cell_id(L + 1, cc)
+                    for m, c3, sub in ((ex & (slo == OUT), lo_c, _E[a]), (ex & (shi == OUT), hi_c, zero)):
+                        kk, jj, ii = np.nonzero(m)
+                        fg = np.stack([ii, jj, kk], axis=1).astype(np.int64)
+                        cc = up.hole_lo + np.floor_divide(fg - sub, 2)
+                        c3[m] = self.cell_id(L + 1, cc)
                 else:                                     # domain boundary families 1..6
-                    fam = np.zeros(fg.shape[0], dtype=np.int8)
-                    lo_side = fg[:, a] == 0
-                    hi_side = fg[:, a] == lv.n[a]
+                    ia = np.arange(fd[a])
+                    fam1 = np.zeros(fd[a], dtype=np.int8)
                     fam_lo, fam_hi = {0: (1, 2), 1: (6, 5), 2: (4, 3)}[a]
-                    fam[lo_side] = fam_lo
-                    fam[hi_side] = fam_hi
-                    self.face_bc[fid] = fam
-                self.face_lo[fid] = np.where(ex, lo_c, -1)
-                self.face_hi[fid] = np.where(ex, hi_c, -1)
+                    fam1[ia == 0] = fam_lo
+                    fam1[ia == lv.n[a]] = fam_hi
+                    shape = [1, 1, 1]
+                    shape[2 - a] = fd[a]
+                    self.face_bc[fs] = np.broadcast_to(fam1.reshape(shape), (fd[2], fd[1], fd[0])).ravel()
+                self.face_lo[fs] = np.where(ex, lo_c, -1).ravel()
+                self.face_hi[fs] = np.where(ex, hi_c, -1).ravel()
                 # edges of axis a
-                eg = _grid(lv.edge_dims(a))
-                eid = self.edge_id(L, a, eg)
+                ed = lv.edge_dims(a)
+                eb = self.edge_base[L][a]
+                es = slice(eb, eb + int(np.prod(ed)))
                 b, c = (a + 1) % 3, (a + 2) % 3
-                sts = np.stack([self.cell_state(L, eg - db * _E[b] - dc * _E[c])
-                                for db in (0, 1) for dc in (0, 1)], axis=1)
-                eex = np.any(sts == ACTIVE, axis=1) & ~np.any(sts == HOLE, axis=1)
-                self.edge_exists[eid] = eex
-                self.edge_axis[eid] = a
-                self.edge_h[eid] = hL
-                self.edge_level[eid] = L
-                self.epos[eid] = lv.lo + hL * (eg + 0.5 * _E[a])
+                any_act = np.zeros((ed[2], ed[1], ed[0]), dtype=bool)
+                any_hole = np.zeros_like(any_act)
+                for db in (0, 1):
+                    for dc in (0, 1):
+                        st = self._state3(L, ed, db * _E[b] + dc * _E[c])
+                        any_act |= st == ACTIVE
+                        any_hole |= st == HOLE
+                self.edge_exists[es] = (any_act & ~any_hole).ravel()
+                self.edge_axis[es] = a
+                self.edge_h[es] = hL
+                self.edge_level[es] = L
+                self._coords3(ed, lv.lo, hL, 0.5 * _E[a], self.epos[es])
             # face-edge links of this level
             for a in range(3):
-                fg = _grid(lv.face_dims(a))
-                fid = self.face_id(L, a, fg)
-                keep = self.face_exists[fid]
-                fg, fid = fg[keep], fid[keep]
+                fd = lv.face_dims(a)
+                fb = self.face_base[L][a]
+                keep = self.face_exists[fb:fb + int(np.prod(fd))]
+                kept = np.flatnonzero(keep)
+                fid = fb + kept
                 b, c = (a + 1) % 3, (a + 2) % 3
-                for ax, off, sgn in ((b, 0, 1.0), (c, _E[b], 1.0), (b, _E[c], -1.0), (c, 0, -1.0)):
-                    eg = fg + off
-                    eid = self.edge_id(L, ax, eg)
+                for ax, off, sgn in ((b, zero, 1.0), (c, _E[b], 1.0), (b, _E[c], -1.0), (c, zero, -1.0)):
+                    eid = self._flat3(fd, self.edge_base[L][ax], -off, lv.edge_dims(ax)).ravel()[kept]
                     ok = self.edge_exists[eid]
                     lk_f.append(fid[ok]); lk_e.append(eid[ok])
                     lk_s.append(np.full(int(ok.sum()), sgn)); lk_x.append(np.zeros(int(ok.sum()), bool))
@@ -251,7 +294,8 @@ class NestedLayout:
                         if L == 0:
                             raise AssertionError("missing edge on the finest level")
                         lvf = self.levels[L - 1]
-                        fine0 = 2 * (eg[~ok] - lv.hole_lo)
+                        eg = _unflat(fd, kept[~ok]) + off
+                        fine0 = 2 * (eg - lv.hole_lo)
                         for j, add in enumerate((0, _E[ax])):
                             sub = self.edge_id(L - 1, ax, fine0 + add)
                             if not np.all(self.edge_exists[sub]) or np.any(fine0 + add < 0) \
