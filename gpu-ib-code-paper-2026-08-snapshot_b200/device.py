@@ -45,12 +45,11 @@ def _rowmap(n, rows):
     return m
 
 
-def _triplets_sorted(rows, cols, vals3, nrows):
-    order = np.lexsort((cols, rows))
-    rows, cols, vals3 = rows[order], cols[order], vals3[order]
-    ptr = np.zeros(nrows + 1, dtype=np.int64)
-    np.add.at(ptr, rows + 1, 1)
-    return np.cumsum(ptr), cols.astype(np.int32), np.ascontiguousarray(vals3, dtype=np.float64)
+def _triplets_sorted(pattern, vals3):
+    """CSR arrays of (row, col, 3 values) entries in row-then-column order, from an
+    entry pattern of ``Operators._pattern``."""
+    order, indptr, indices = pattern
+    return indptr.copy(), indices.astype(np.int32), np.ascontiguousarray(vals3[order], dtype=np.float64)
 
 
 class LayoutTables:
@@ -99,25 +98,19 @@ class LayoutTables:
         A["INLET_VAL"] = lay.epos[ie, 1] * hz
         for name, M in (("CURL", ops.C), ("ROT", ops.R)):
             A[name + "_PTR"], A[name + "_COL"], A[name + "_VAL"] = _csr_arrays(M)
-        f = np.nonzero(lay.face_exists)[0]
-        lo, hi = lay.face_lo[f], lay.face_hi[f]
-        mlo, mhi = lo >= 0, hi >= 0
+        fc = ops.faces
+        f, lo, hi, mlo, mhi, dlo, dhi = (fc[k] for k in ("f", "lo", "hi", "mlo", "mhi", "dlo", "dhi"))
         vol_ci = ops.vol_ci
-        dlo = lay.fpos[f[mlo]] - lay.cpos[lo[mlo]]
-        dhi = lay.fpos[f[mhi]] - lay.cpos[hi[mhi]]
-        # interp_f2c: rows cells, cols faces, 3 values
-        rows = np.concatenate([lo[mlo], hi[mhi]])
-        cols = np.concatenate([f[mlo], f[mhi]])
+        # interp_f2c: rows cells, cols faces, 3 values (the operators' cell x face order)
         v3 = np.concatenate([vol_ci[lo[mlo], None] * dlo, -vol_ci[hi[mhi], None] * dhi])
-        A["P_PTR"], A["P_COL"], A["P_VAL3"] = _triplets_sorted(rows, cols, v3, NC)
+        A["P_PTR"], A["P_COL"], A["P_VAL3"] = _triplets_sorted(ops.cf, v3)
         # integr_c2f: rows faces, cols cells
-        A["I_PTR"], A["I_COL"], A["I_VAL3"] = _triplets_sorted(cols, rows, np.concatenate([dlo, -dhi]), NF)
-        # cell -> signed faces (bit 0 set: the face's +a side is this cell)
+        A["I_PTR"], A["I_COL"], A["I_VAL3"] = _triplets_sorted(ops.fc, np.concatenate([dlo, -dhi]))
+        # cell -> signed faces (bit 0 set: the face's +a side is this cell), by cell and
+        # then face: the cell x face order, since 2 face + side grows with the face
         code = np.concatenate([(f[mlo] << 1), (f[mhi] << 1) | 1]).astype(np.int64)
-        order = np.lexsort((code, rows))
-        ptr = np.zeros(NC + 1, dtype=np.int64)
-        np.add.at(ptr, rows + 1, 1)
-        A["CF_PTR"] = np.cumsum(ptr)
+        order, indptr, _ = ops.cf
+        A["CF_PTR"] = indptr.copy()
         A["CF_FACE"] = code[order].astype(np.int32)
         # face cells with ghost slots
         bf = self.bfaces

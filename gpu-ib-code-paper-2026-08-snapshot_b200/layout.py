@@ -198,6 +198,7 @@ class NestedLayout:
         per-axis 1D tests.
         """
         NC, NF, NE = self.NC, self.NF, self.NE
+        self._rf = None
         self.cell_active = np.zeros(NC, dtype=bool)
         self.cell_h = np.zeros(NC)
         self.cpos = np.zeros((NC, 3))
@@ -318,7 +319,14 @@ class NestedLayout:
 
     # ---- geometry needed by the operators ---------------------------------
     def face_rf(self):
-        """rf = (cpos_hi or fpos) - (cpos_lo or fpos), the +a oriented centre-to-centre vector."""
+        """rf = (cpos_hi or fpos) - (cpos_lo or fpos), the +a oriented centre-to-centre vector
+        (computed once per built layout; callers must not modify it)."""
+        if getattr(self, "_rf", None) is not None:
+            return self._rf
+        self._rf = self._face_rf()
+        return self._rf
+
+    def _face_rf(self):
         lo, hi = self.face_lo, self.face_hi
         a = np.where(lo >= 0, 0, 1)
         plo = np.where((lo >= 0)[:, None], self.cpos[np.maximum(lo, 0)], self.fpos)

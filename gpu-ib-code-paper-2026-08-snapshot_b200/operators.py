@@ -39,22 +39,39 @@ class Operators:
         self.vol_ci = vol_ci
         dlo = lay.fpos[f[mlo]] - lay.cpos[lo[mlo]]
         dhi = lay.fpos[f[mhi]] - lay.cpos[hi[mhi]]
+        # cell-face incidence entries (the -a side cells first), and the two orders
+        # that list them as rows of cells x faces and of faces x cells
+        rows = np.concatenate([lo[mlo], hi[mhi]])
+        cols = np.concatenate([f[mlo], f[mhi]])
+        self.cf = self._pattern(rows, cols, NC)
+        self.fc = self._pattern(cols, rows, NF)
+        self.faces = dict(f=f, lo=lo, hi=hi, mlo=mlo, mhi=mhi, dlo=dlo, dhi=dhi, rows=rows, cols=cols)
         self.P, self.I = [], []
         for d in range(3):
-            rows = np.concatenate([lo[mlo], hi[mhi]])
-            cols = np.concatenate([f[mlo], f[mhi]])
             vals = np.concatenate([vol_ci[lo[mlo]] * dlo[:, d], -vol_ci[hi[mhi]] * dhi[:, d]])
-            self.P.append(sp.csr_matrix((vals, (rows, cols)), shape=(NC, NF)))
-            self.I.append(sp.csr_matrix((np.concatenate([dlo[:, d], -dhi[:, d]]), (cols, rows)),
-                                        shape=(NF, NC)))
-        self.D = sp.csr_matrix((np.concatenate([np.ones(mlo.sum()), -np.ones(mhi.sum())]),
-                                (np.concatenate([lo[mlo], hi[mhi]]), np.concatenate([f[mlo], f[mhi]]))),
-                               shape=(NC, NF))
-        self.G0 = sp.csr_matrix((np.concatenate([-np.ones(mlo.sum()), np.ones(mhi.sum())]),
-                                 (np.concatenate([f[mlo], f[mhi]]), np.concatenate([lo[mlo], hi[mhi]]))),
-                                shape=(NF, NC))
+            self.P.append(self._csr(self.cf, vals, (NC, NF)))
+            self.I.append(self._csr(self.fc, np.concatenate([dlo[:, d], -dhi[:, d]]), (NF, NC)))
+        self.D = self._csr(self.cf, np.concatenate([np.ones(mlo.sum()), -np.ones(mhi.sum())]), (NC, NF))
+        self.G0 = self._csr(self.fc, np.concatenate([-np.ones(mlo.sum()), np.ones(mhi.sum())]), (NF, NC))
         self.AoL = lay.face_AoL()
         self.Vd = (sp.diags(vol_ci) @ self.D @ sp.diags(self.AoL) @ self.G0).tocsr()
+
+    @staticmethod
+    def _pattern(rows, cols, nrows):
+        """(order, indptr, indices) listing the entries (rows, cols) by row and then
+        column: the canonical CSR of scipy's COO conversion, for entries without
+        duplicate (row, column) pairs, computed once per pattern."""
+        key = (rows.astype(np.int64) << 32) | cols.astype(np.int64)
+        order = np.argsort(key, kind="stable")
+        indptr = np.zeros(nrows + 1, dtype=np.int64)
+        np.cumsum(np.bincount(rows, minlength=nrows), out=indptr[1:])
+        return order, indptr, cols[order]
+
+    @staticmethod
+    def _csr(pattern, vals, shape):
+        order, indptr, indices = pattern
+        idx_t = np.int32 if max(shape) < 2**31 and indices.size < 2**31 else np.int64
+        return sp.csr_matrix((vals[order], indices.astype(idx_t), indptr.astype(idx_t)), shape=shape)
 
     # ---- boundary conditions (ib_driver_np.py:120-121, 155-166) -----------
     def dir_mask(self, cavity):

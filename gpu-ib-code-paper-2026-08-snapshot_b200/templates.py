@@ -23,6 +23,8 @@ compare the kernels with them and with the exact operators.
 """
 from __future__ import annotations
 
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import scipy.sparse as sp
 
@@ -169,24 +171,42 @@ class MatvecPlan:
         self.mask = lay.edge_exists & ~dir_mask
         rng = np.random.default_rng(seed)
         act = lay.cell_active
-        irrA = np.zeros(lay.NC, dtype=bool)
-        irrV = np.zeros(lay.NC, dtype=bool)
-        irrRI = np.zeros(lay.NE, dtype=bool)
+        # the probe vectors, drawn in a fixed order; the comparisons of the three
+        # stages run on host threads (the array and sparse kernels release the
+        # interpreter lock) and their flags are or-ed, so the result is the same
+        draws = []
         for _ in range(probes):
             p = rng.standard_normal(lay.NE)
+            v = rng.standard_normal(lay.NC)
+            vq = rng.standard_normal((3, lay.NC))
+            draws.append((p, v, vq))
+
+        def stage_a(p):
             U = ops.C @ p
             ex = np.stack([ops.P[d] @ U for d in range(3)])
-            irrA |= np.any(_differs(t_A(lay, p), ex), axis=0) & act
-            v = rng.standard_normal(lay.NC)
+            return np.any(_differs(t_A(lay, p), ex), axis=0) & act
+
+        def stage_v(v):
             # rou=0, visc=2, dt=1 -> template computes -(Vd v)
-            irrV |= _differs(t_V(lay, v, 0.0, 2.0, 1.0), -(ops.Vd @ v)) & act
-            vq = rng.standard_normal((3, lay.NC))
+            return _differs(t_V(lay, v, 0.0, 2.0, 1.0), -(ops.Vd @ v)) & act
+
+        def stage_ri(vq):
             exw = ops.R @ sum(ops.I[d] @ vq[d] for d in range(3))
-            irrRI |= _differs(t_RI(lay, vq), exw) & self.mask
+            return _differs(t_RI(lay, vq), exw) & self.mask
+
+        with ThreadPoolExecutor(max_workers=min(6, 3 * probes)) as pool:
+            fa = [pool.submit(stage_a, p) for p, _, _ in draws]
+            fv = [pool.submit(stage_v, v) for _, v, _ in draws]
+            fr = [pool.submit(stage_ri, vq) for _, _, vq in draws]
+            upper = pool.submit(upper_face_edges, lay)
+            irrA = np.logical_or.reduce([x.result() for x in fa])
+            irrV = np.logical_or.reduce([x.result() for x in fv])
+            irrRI = np.logical_or.reduce([x.result() for x in fr])
+            upper = upper.result()
         # the edges of the nodes on a level's upper faces (i = nx, j = ny or k = nz) are
         # interface or boundary edges; when every one of them is already an exact row or
         # masked (closed cavities), the RI kernel covers only nodes i < nx, j < ny, k < nz
-        self.upper_exact = not np.any(upper_face_edges(lay) & self.mask & ~irrRI)
+        self.upper_exact = not np.any(upper & self.mask & ~irrRI)
         self.irrA, self.irrV, self.irrRI = irrA, irrV, irrRI
         ra = np.nonzero(irrA)[0]
         # exact composite rows: component-major blocks of the same cell list
@@ -230,9 +250,11 @@ def upper_face_edges(lay):
     out = np.zeros(lay.NE, dtype=bool)
     for lv in lay.levels:
         for a in range(3):
-            g = _grid(lv.edge_dims(a))
-            up = np.any(g == lv.n, axis=1)
-            out[lay.edge_id(lv.L, a, g[up])] = True
+            ed = lv.edge_dims(a)
+            i, j, k = (np.arange(ed[t]) == lv.n[t] for t in range(3))
+            up = k[:, None, None] | j[None, :, None] | i[None, None, :]
+            eb = lay.edge_base[lv.L][a]
+            out[eb:eb + up.size] = up.ravel()
     return out
 
 
