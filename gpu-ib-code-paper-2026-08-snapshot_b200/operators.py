@@ -47,12 +47,13 @@ class Operators:
         self.fc = self._pattern(cols, rows, NF)
         self.faces = dict(f=f, lo=lo, hi=hi, mlo=mlo, mhi=mhi, dlo=dlo, dhi=dhi, rows=rows, cols=cols)
         self.P, self.I = [], []
+        ccf, cfc = {}, {}
         for d in range(3):
             vals = np.concatenate([vol_ci[lo[mlo]] * dlo[:, d], -vol_ci[hi[mhi]] * dhi[:, d]])
-            self.P.append(self._csr(self.cf, vals, (NC, NF)))
-            self.I.append(self._csr(self.fc, np.concatenate([dlo[:, d], -dhi[:, d]]), (NF, NC)))
-        self.D = self._csr(self.cf, np.concatenate([np.ones(mlo.sum()), -np.ones(mhi.sum())]), (NC, NF))
-        self.G0 = self._csr(self.fc, np.concatenate([-np.ones(mlo.sum()), np.ones(mhi.sum())]), (NF, NC))
+            self.P.append(self._csr(self.cf, vals, (NC, NF), ccf))
+            self.I.append(self._csr(self.fc, np.concatenate([dlo[:, d], -dhi[:, d]]), (NF, NC), cfc))
+        self.D = self._csr(self.cf, np.concatenate([np.ones(mlo.sum()), -np.ones(mhi.sum())]), (NC, NF), ccf)
+        self.G0 = self._csr(self.fc, np.concatenate([-np.ones(mlo.sum()), np.ones(mhi.sum())]), (NF, NC), cfc)
         self.AoL = lay.face_AoL()
         self.Vd = (sp.diags(vol_ci) @ self.D @ sp.diags(self.AoL) @ self.G0).tocsr()
 
@@ -68,10 +69,16 @@ class Operators:
         return order, indptr, cols[order]
 
     @staticmethod
-    def _csr(pattern, vals, shape):
+    def _csr(pattern, vals, shape, cache):
+        """CSR of ``vals`` on a pattern.  The index arrays, in the index type scipy
+        picks for the size, are converted once (``cache``, one per pattern) and
+        shared by the pattern's matrices."""
         order, indptr, indices = pattern
         idx_t = np.int32 if max(shape) < 2**31 and indices.size < 2**31 else np.int64
-        return sp.csr_matrix((vals[order], indices.astype(idx_t), indptr.astype(idx_t)), shape=shape)
+        if idx_t not in cache:
+            cache[idx_t] = (indices.astype(idx_t), indptr.astype(idx_t))
+        ind, ptr = cache[idx_t]
+        return sp.csr_matrix((vals[order], ind, ptr), shape=shape)
 
     # ---- boundary conditions (ib_driver_np.py:120-121, 155-166) -----------
     def dir_mask(self, cavity):
