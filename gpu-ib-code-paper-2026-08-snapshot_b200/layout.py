@@ -36,6 +36,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 
 OUT, ACTIVE, HOLE = 0, 1, 2
@@ -190,6 +192,102 @@ class NestedLayout:
         o[..., 1] = (lo[1] + h * (np.arange(dims[1]) + shift[1]))[None, :, None]
         o[..., 2] = (lo[2] + h * (np.arange(dims[2]) + shift[2]))[:, None, None]
 
+    def _build_level(self, lv):
+        """Cells, faces and edges of one level (disjoint slices of every table)."""
+        zero = np.zeros(3, dtype=np.int64)
+        L, hL = lv.L, lv.h
+        cb = self.cell_base[L]
+        ncl = int(np.prod(lv.n))
+        cs = slice(cb, cb + ncl)
+        self.cell_active[cs] = (self._state3(L, lv.n, zero) == ACTIVE).ravel()
+        self.cell_h[cs] = hL
+        self.cell_level[cs] = L
+        self._coords3(lv.n, lv.lo, hL, (0.5, 0.5, 0.5), self.cpos[cs])
+        for a in range(3):
+            # faces of axis a
+            fd = lv.face_dims(a)
+            fb = self.face_base[L][a]
+            fs = slice(fb, fb + int(np.prod(fd)))
+            slo = self._state3(L, fd, _E[a])
+            shi = self._state3(L, fd, zero)
+            ex = ((slo == ACTIVE) & (shi == ACTIVE)) | ((slo == ACTIVE) & (shi == OUT)) \
+                | ((slo == OUT) & (shi == ACTIVE))
+            self.face_exists[fs] = ex.ravel()
+            self.face_axis[fs] = a
+            self.face_h[fs] = hL
+            self.face_level[fs] = L
+            self._coords3(fd, lv.lo, hL, 0.5 * (1 - _E[a]), self.fpos[fs])
+            lo_c = np.where(slo == ACTIVE, self._flat3(fd, cb, _E[a], lv.n), -1)
+            hi_c = np.where(shi == ACTIVE, self._flat3(fd, cb, zero, lv.n), -1)
+            if L + 1 < self.N:                        # interface faces: coarse neighbour
+                up = self.levels[L + 1]
+                for m, c3, sub in ((ex & (slo == OUT), lo_c, _E[a]), (ex & (shi == OUT), hi_c, zero)):
+                    kk, jj, ii = np.nonzero(m)
+                    fg = np.stack([ii, jj, kk], axis=1).astype(np.int64)
+                    cc = up.hole_lo + np.floor_divide(fg - sub, 2)
+                    c3[m] = self.cell_id(L + 1, cc)
+            else:                                     # domain boundary families 1..6
+                ia = np.arange(fd[a])
+                fam1 = np.zeros(fd[a], dtype=np.int8)
+                fam_lo, fam_hi = {0: (1, 2), 1: (6, 5), 2: (4, 3)}[a]
+                fam1[ia == 0] = fam_lo
+                fam1[ia == lv.n[a]] = fam_hi
+                shape = [1, 1, 1]
+                shape[2 - a] = fd[a]
+                self.face_bc[fs] = np.broadcast_to(fam1.reshape(shape), (fd[2], fd[1], fd[0])).ravel()
+            self.face_lo[fs] = np.where(ex, lo_c, -1).ravel()
+            self.face_hi[fs] = np.where(ex, hi_c, -1).ravel()
+            # edges of axis a
+            ed = lv.edge_dims(a)
+            eb = self.edge_base[L][a]
+            es = slice(eb, eb + int(np.prod(ed)))
+            b, c = (a + 1) % 3, (a + 2) % 3
+            any_act = np.zeros((ed[2], ed[1], ed[0]), dtype=bool)
+            any_hole = np.zeros_like(any_act)
+            for db in (0, 1):
+                for dc in (0, 1):
+                    st = self._state3(L, ed, db * _E[b] + dc * _E[c])
+                    any_act |= st == ACTIVE
+                    any_hole |= st == HOLE
+            self.edge_exists[es] = (any_act & ~any_hole).ravel()
+            self.edge_axis[es] = a
+            self.edge_h[es] = hL
+            self.edge_level[es] = L
+            self._coords3(ed, lv.lo, hL, 0.5 * _E[a], self.epos[es])
+
+    def _level_links(self, lv):
+        """Face-edge links of one level's faces, in face order (needs the edges of
+        this level and of the finer one)."""
+        L = lv.L
+        zero = np.zeros(3, dtype=np.int64)
+        lk_f, lk_e, lk_s, lk_x = [], [], [], []
+        for a in range(3):
+            fd = lv.face_dims(a)
+            fb = self.face_base[L][a]
+            keep = self.face_exists[fb:fb + int(np.prod(fd))]
+            kept = np.flatnonzero(keep)
+            fid = fb + kept
+            b, c = (a + 1) % 3, (a + 2) % 3
+            for ax, off, sgn in ((b, zero, 1.0), (c, _E[b], 1.0), (b, _E[c], -1.0), (c, zero, -1.0)):
+                eid = self._flat3(fd, self.edge_base[L][ax], -off, lv.edge_dims(ax)).ravel()[kept]
+                ok = self.edge_exists[eid]
+                lk_f.append(fid[ok]); lk_e.append(eid[ok])
+                lk_s.append(np.full(int(ok.sum()), sgn)); lk_x.append(np.zeros(int(ok.sum()), bool))
+                if not np.all(ok):                    # collapsed coarse edge -> 2 fine sub-edges
+                    if L == 0:
+                        raise AssertionError("missing edge on the finest level")
+                    lvf = self.levels[L - 1]
+                    eg = _unflat(fd, kept[~ok]) + off
+                    fine0 = 2 * (eg - lv.hole_lo)
+                    for j, add in enumerate((0, _E[ax])):
+                        sub = self.edge_id(L - 1, ax, fine0 + add)
+                        if not np.all(self.edge_exists[sub]) or np.any(fine0 + add < 0) \
+                                or np.any(fine0 + add >= lvf.edge_dims(ax)):
+                            raise AssertionError("collapsed edge without fine sub-edges")
+                        lk_f.append(fid[~ok]); lk_e.append(sub)
+                        lk_s.append(np.full(sub.size, sgn)); lk_x.append(np.full(sub.size, j == 1))
+        return lk_f, lk_e, lk_s, lk_x
+
     def build(self):
         """Existence masks, face cells, face-edge links and geometry (dense ids).
 
@@ -216,94 +314,16 @@ class NestedLayout:
         self.edge_level = np.zeros(NE, dtype=np.int8)
         self.face_level = np.zeros(NF, dtype=np.int8)
         self.cell_level = np.zeros(NC, dtype=np.int8)
-        lk_f, lk_e, lk_s, lk_x = [], [], [], []          # face-edge links (x: extra link)
-        zero = np.zeros(3, dtype=np.int64)
-        for lv in self.levels:
-            L, hL = lv.L, lv.h
-            cb = self.cell_base[L]
-            ncl = int(np.prod(lv.n))
-            cs = slice(cb, cb + ncl)
-            self.cell_active[cs] = (self._state3(L, lv.n, zero) == ACTIVE).ravel()
-            self.cell_h[cs] = hL
-            self.cell_level[cs] = L
-            self._coords3(lv.n, lv.lo, hL, (0.5, 0.5, 0.5), self.cpos[cs])
-            for a in range(3):
-                # faces of axis a
-                fd = lv.face_dims(a)
-                fb = self.face_base[L][a]
-                fs = slice(fb, fb + int(np.prod(fd)))
-                slo = self._state3(L, fd, _E[a])
-                shi = self._state3(L, fd, zero)
-                ex = ((slo == ACTIVE) & (shi == ACTIVE)) | ((slo == ACTIVE) & (shi == OUT)) \
-                    | ((slo == OUT) & (shi == ACTIVE))
-                self.face_exists[fs] = ex.ravel()
-                self.face_axis[fs] = a
-                self.face_h[fs] = hL
-                self.face_level[fs] = L
-                self._coords3(fd, lv.lo, hL, 0.5 * (1 - _E[a]), self.fpos[fs])
-                lo_c = np.where(slo == ACTIVE, self._flat3(fd, cb, _E[a], lv.n), -1)
-                hi_c = np.where(shi == ACTIVE, self._flat3(fd, cb, zero, lv.n), -1)
-                if L + 1 < self.N:                        # interface faces: coarse neighbour
-                    up = self.levels[L + 1]
-                    for m, c3, sub in ((ex & (slo == OUT), lo_c, _E[a]), (ex & (shi == OUT), hi_c, zero)):
-                        kk, jj, ii = np.nonzero(m)
-                        fg = np.stack([ii, jj, kk], axis=1).astype(np.int64)
-                        cc = up.hole_lo + np.floor_divide(fg - sub, 2)
-                        c3[m] = self.cell_id(L + 1, cc)
-                else:                                     # domain boundary families 1..6
-                    ia = np.arange(fd[a])
-                    fam1 = np.zeros(fd[a], dtype=np.int8)
-                    fam_lo, fam_hi = {0: (1, 2), 1: (6, 5), 2: (4, 3)}[a]
-                    fam1[ia == 0] = fam_lo
-                    fam1[ia == lv.n[a]] = fam_hi
-                    shape = [1, 1, 1]
-                    shape[2 - a] = fd[a]
-                    self.face_bc[fs] = np.broadcast_to(fam1.reshape(shape), (fd[2], fd[1], fd[0])).ravel()
-                self.face_lo[fs] = np.where(ex, lo_c, -1).ravel()
-                self.face_hi[fs] = np.where(ex, hi_c, -1).ravel()
-                # edges of axis a
-                ed = lv.edge_dims(a)
-                eb = self.edge_base[L][a]
-                es = slice(eb, eb + int(np.prod(ed)))
-                b, c = (a + 1) % 3, (a + 2) % 3
-                any_act = np.zeros((ed[2], ed[1], ed[0]), dtype=bool)
-                any_hole = np.zeros_like(any_act)
-                for db in (0, 1):
-                    for dc in (0, 1):
-                        st = self._state3(L, ed, db * _E[b] + dc * _E[c])
-                        any_act |= st == ACTIVE
-                        any_hole |= st == HOLE
-                self.edge_exists[es] = (any_act & ~any_hole).ravel()
-                self.edge_axis[es] = a
-                self.edge_h[es] = hL
-                self.edge_level[es] = L
-                self._coords3(ed, lv.lo, hL, 0.5 * _E[a], self.epos[es])
-            # face-edge links of this level
-            for a in range(3):
-                fd = lv.face_dims(a)
-                fb = self.face_base[L][a]
-                keep = self.face_exists[fb:fb + int(np.prod(fd))]
-                kept = np.flatnonzero(keep)
-                fid = fb + kept
-                b, c = (a + 1) % 3, (a + 2) % 3
-                for ax, off, sgn in ((b, zero, 1.0), (c, _E[b], 1.0), (b, _E[c], -1.0), (c, zero, -1.0)):
-                    eid = self._flat3(fd, self.edge_base[L][ax], -off, lv.edge_dims(ax)).ravel()[kept]
-                    ok = self.edge_exists[eid]
-                    lk_f.append(fid[ok]); lk_e.append(eid[ok])
-                    lk_s.append(np.full(int(ok.sum()), sgn)); lk_x.append(np.zeros(int(ok.sum()), bool))
-                    if not np.all(ok):                    # collapsed coarse edge -> 2 fine sub-edges
-                        if L == 0:
-                            raise AssertionError("missing edge on the finest level")
-                        lvf = self.levels[L - 1]
-                        eg = _unflat(fd, kept[~ok]) + off
-                        fine0 = 2 * (eg - lv.hole_lo)
-                        for j, add in enumerate((0, _E[ax])):
-                            sub = self.edge_id(L - 1, ax, fine0 + add)
-                            if not np.all(self.edge_exists[sub]) or np.any(fine0 + add < 0) \
-                                    or np.any(fine0 + add >= lvf.edge_dims(ax)):
-                                raise AssertionError("collapsed edge without fine sub-edges")
-                            lk_f.append(fid[~ok]); lk_e.append(sub)
-                            lk_s.append(np.full(sub.size, sgn)); lk_x.append(np.full(sub.size, j == 1))
+        # levels fill disjoint slices, so they are built on host threads (the array
+        # kernels release the interpreter lock); the links of each level, which
+        # read the finer level's edges, follow, concatenated in level order
+        with ThreadPoolExecutor(max_workers=max(1, min(4, self.N))) as pool:
+            list(pool.map(self._build_level, self.levels))
+            parts = list(pool.map(self._level_links, self.levels))
+        lk_f = [x for pt in parts for x in pt[0]]
+        lk_e = [x for pt in parts for x in pt[1]]
+        lk_s = [x for pt in parts for x in pt[2]]
+        lk_x = [x for pt in parts for x in pt[3]]
         self.link_face = np.concatenate(lk_f)
         self.link_edge = np.concatenate(lk_e)
         self.link_sign = np.concatenate(lk_s)

@@ -18,6 +18,8 @@ structured templates cannot reproduce become explicit patch rows.
 """
 from __future__ import annotations
 
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import scipy.sparse as sp
 
@@ -28,9 +30,25 @@ class Operators:
             lay.build()
         self.lay = lay
         NC, NF, NE = lay.NC, lay.NF, lay.NE
-        self.C = sp.csr_matrix((lay.link_sign, (lay.link_face, lay.link_edge)), shape=(NF, NE))
-        self.C.sum_duplicates()
-        self.R = self.C.T.tocsr()
+
+        def curl():
+            C = sp.csr_matrix((lay.link_sign, (lay.link_face, lay.link_edge)), shape=(NF, NE))
+            C.sum_duplicates()
+            return C, C.T.tocsr()
+
+        # the curl pair and the face geometry are independent of the cell-face
+        # matrices below: they are built on host threads meanwhile (the array and
+        # sparse kernels release the interpreter lock; the values do not change)
+        with ThreadPoolExecutor(max_workers=2) as pool:
+            f_curl = pool.submit(curl)
+            f_aol = pool.submit(lay.face_AoL)
+            self._cell_face(lay, NC, NF)
+            self.C, self.R = f_curl.result()
+            self.AoL = f_aol.result()
+        self.Vd = (sp.diags(self.vol_ci) @ self.D @ sp.diags(self.AoL) @ self.G0).tocsr()
+
+    def _cell_face(self, lay, NC, NF):
+        """P, I, D, G0 and the face data and entry orders they share."""
         f = np.nonzero(lay.face_exists)[0]
         lo, hi = lay.face_lo[f], lay.face_hi[f]
         mlo, mhi = lo >= 0, hi >= 0
@@ -54,8 +72,6 @@ class Operators:
             self.I.append(self._csr(self.fc, np.concatenate([dlo[:, d], -dhi[:, d]]), (NF, NC), cfc))
         self.D = self._csr(self.cf, np.concatenate([np.ones(mlo.sum()), -np.ones(mhi.sum())]), (NC, NF), ccf)
         self.G0 = self._csr(self.fc, np.concatenate([-np.ones(mlo.sum()), np.ones(mhi.sum())]), (NF, NC), cfc)
-        self.AoL = lay.face_AoL()
-        self.Vd = (sp.diags(vol_ci) @ self.D @ sp.diags(self.AoL) @ self.G0).tocsr()
 
     @staticmethod
     def _pattern(rows, cols, nrows):
