@@ -151,3 +151,36 @@ def test_device_assembly_matches_host_assembly():
     q -= q[boundary].mean()
     assert np.max(np.abs(p - q)) <= 1e-9 * np.max(np.abs(q))
     assert abs(it - diag["iterations"]) <= 2
+
+
+def test_edge_cases_match_oracle():
+    """The smallest graph, duplicate faces between one pair of cells (summed in the
+    reference's Laplacian, kept as separate entries here), and unsigned face ids
+    with no boundary face (gauge: the mean over all cells)."""
+    rng = np.random.default_rng(21)
+    # two cells, one internal face, two boundary faces
+    pos = np.array([[0.0, 0.0, 0.0], [0.5, 0.0, 0.0]])
+    faces = np.array([[0, 1], [0, -1], [1, -1]])
+    grad = rng.standard_normal((2, 3))
+    p, d = PP.recover_pressure(pos, faces, np.ones(3), grad)
+    q, e = PO.recover_pressure(pos, faces, np.ones(3), grad)
+    np.testing.assert_allclose(p, q, rtol=0, atol=1e-14)
+    assert d["gauge"] == e["gauge"] == "mean boundary-adjacent cells = 0"
+    # duplicate faces on a 6^3 lattice: every x face listed twice with split areas
+    pos, faces, area = PO.uniform_graph(6, 0.25)
+    xf = (faces[:, 1] >= 0) & (pos[np.maximum(faces[:, 1], 0), 0] != pos[faces[:, 0], 0])
+    faces2 = np.concatenate([faces, faces[xf]])
+    area2 = np.concatenate([np.where(xf, 0.25 * area, area), 0.75 * area[xf]])
+    grad = PO.quadratic_gradient(pos) + 0.05 * rng.standard_normal(pos.shape)
+    p, d = PP.recover_pressure(pos, faces2, area2, grad)
+    q, e = PO.recover_pressure(pos, faces2, area2, grad)
+    assert np.max(np.abs(p - q)) <= 1e-9 * np.max(np.abs(q))
+    assert abs(d["gradient_projection_weighted_rms"] - e["gradient_projection_weighted_rms"]) <= \
+        1e-8 * e["gradient_projection_weighted_rms"]
+    # unsigned ids, internal faces only
+    inner = faces[faces[:, 1] >= 0].astype(np.uint32)
+    p, d = PP.recover_pressure(pos, inner, np.ones(len(inner)), grad)
+    q, e = PO.recover_pressure(pos, inner, np.ones(len(inner)), grad)
+    assert d["gauge"] == e["gauge"] == "mean cells = 0"
+    assert abs(p.mean()) < 1e-14
+    assert np.max(np.abs(p - q)) <= 1e-9 * np.max(np.abs(q))
