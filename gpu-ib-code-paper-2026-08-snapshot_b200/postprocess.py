@@ -23,6 +23,7 @@ not part of this module.
 from __future__ import annotations
 
 import ctypes as C
+import threading
 
 import numpy as np
 from scipy.sparse import csr_matrix
@@ -41,8 +42,9 @@ def _finite(name, values, shape=None):
 
 
 def bare_handle(device=0):
-    """A context with a one-cell layout: a device, a stream and an error slot for
-    the calls that take all their data from the caller (``pyib_graph_pcg``)."""
+    """A context with a one-cell layout: a device, a stream, an error slot and a
+    grow-only workspace for the calls that take all their data from the caller
+    (``pyib_recover_pressure``, ``pyib_graph_pcg``)."""
     lay = _lib.Layout()
     lay.nlevels = 1
     lay.n[0][0] = lay.n[0][1] = lay.n[0][2] = 1
@@ -50,6 +52,22 @@ def bare_handle(device=0):
     lay.ncell, lay.nface, lay.nedge = 1, 6, 12
     lay.device = int(device)
     return _lib.Handle(lay)
+
+
+_local = threading.local()
+
+
+def default_handle(device=0):
+    """This host thread's context on ``device`` for calls made without a handle:
+    made on first use and kept, so its workspace is reused by later calls (one
+    context per host thread, as the library requires)."""
+    handles = getattr(_local, "handles", None)
+    if handles is None:
+        handles = _local.handles = {}
+    h = handles.get(int(device))
+    if h is None or not h.ptr:
+        h = handles[int(device)] = bare_handle(device)
+    return h
 
 
 def laplacian_csr(count, first, second, weights):
@@ -159,8 +177,9 @@ def recover_pressure(cell_positions, face_cells, face_area, gradient, *, toleran
     disconnected input, RuntimeError when the solve does not converge).  Shapes and
     types are checked here; the value checks, the assembly, the connectivity check,
     the CG, the gauge and the residual run on the device (``pyib_recover_pressure``).
-    ``handle`` reuses an existing context (a solver's ``h``); otherwise one is made
-    on ``device``.  The diagnostics add ``iterations``; ``timing`` (a dict) receives
+    ``handle`` reuses an existing context (a solver's ``h``); otherwise this host
+    thread's context on ``device`` is used (``default_handle``).  The diagnostics
+    add ``iterations``; ``timing`` (a dict) receives
     ``solve_ms`` (the CG), ``device_ms`` (the whole call on the device, copies
     included), ``sweeps`` (connectivity) and ``nnz``.
     """
@@ -183,23 +202,18 @@ def recover_pressure(cell_positions, face_cells, face_area, gradient, *, toleran
     max_it = max(2000, 10 * count)
     out = np.empty(count)
     info = np.zeros(7)
-    own = handle is None
-    h = bare_handle(device) if own else handle
-    try:
-        rc = h.lib.pyib_recover_pressure(
-            h.ptr, C.c_int64(count), pos.ctypes.data_as(C.c_void_p), C.c_int64(len(pairs64)),
-            pairs64.ctypes.data_as(C.c_void_p), area.ctypes.data_as(C.c_void_p), grad.ctypes.data_as(C.c_void_p),
-            C.c_double(tolerance), C.c_int32(int(max_it)), out.ctypes.data_as(C.c_void_p),
-            info.ctypes.data_as(C.c_void_p))
-        if rc == _lib.E_ARG:
-            raise ValueError(h.error())
-        if rc == _lib.E_NOCONV:
-            raise RuntimeError(h.error())
-        if rc != _lib.OK:
-            raise _lib.B200Error(rc, f"pyib_recover_pressure: {h.error()}")
-    finally:
-        if own:
-            h.close()
+    h = default_handle(device) if handle is None else handle
+    rc = h.lib.pyib_recover_pressure(
+        h.ptr, C.c_int64(count), pos.ctypes.data_as(C.c_void_p), C.c_int64(len(pairs64)),
+        pairs64.ctypes.data_as(C.c_void_p), area.ctypes.data_as(C.c_void_p), grad.ctypes.data_as(C.c_void_p),
+        C.c_double(tolerance), C.c_int32(int(max_it)), out.ctypes.data_as(C.c_void_p),
+        info.ctypes.data_as(C.c_void_p))
+    if rc == _lib.E_ARG:
+        raise ValueError(h.error())
+    if rc == _lib.E_NOCONV:
+        raise RuntimeError(h.error())
+    if rc != _lib.OK:
+        raise _lib.B200Error(rc, f"pyib_recover_pressure: {h.error()}")
     if timing is not None:
         timing.update(solve_ms=float(info[3]), device_ms=float(info[4]), sweeps=int(info[5]), nnz=int(info[6]))
     diagnostics = {
