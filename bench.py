@@ -552,56 +552,97 @@ def run_harmonic(args, world, rank, local):
 # ---------------------------------------------------------------------------
 # Batched sweep: independent cases of uneven size, concurrent vs one at a time
 # ---------------------------------------------------------------------------
+def aggregate_batch(dist, seconds_concurrent, seconds_sequential, cells, launches, cg_iterations,
+                    max_case_iterations):
+    """Whole-job figures of a sharded sweep: the slowest rank's times, the sums of
+    the per-rank work (every rank calls the same reductions in the same order)."""
+    return {
+        "seconds_concurrent": reduce_max(dist, float(seconds_concurrent)),
+        "seconds_sequential": reduce_max(dist, float(seconds_sequential)),
+        "cells": reduce_sum(dist, float(cells)),
+        "launches": reduce_sum(dist, float(launches)),
+        "cg_iterations": reduce_sum(dist, float(cg_iterations)),
+        "max_case_iterations": reduce_max(dist, float(max_case_iterations)),
+    }
+
+
 def run_batch(args, world, rank, local):
     """Aggregate cell-updates/s of the seeded sweep, concurrently and one case at a time.
 
     Both timings advance every case by ``--steps`` steps (consecutive steps of the
     same runs: first concurrently, then sequentially); host wall clock around
-    each phase, every case's last call having waited for its own stream.
+    each phase, every case's last call having waited for its own stream.  Under
+    torchrun the cases are split across the ranks by cost (cells x steps,
+    longest first, ``batch.partition``): each rank runs its own share with no
+    collective on the data path, and the line reports the summed work over the
+    slowest rank's time.
     """
+    from collections import Counter
+
     import _pyib_b200_import
     _pyib_b200_import.load()
     from pyib_b200 import build
-    from pyib_b200.batch import BatchRun, sweep_cases
+    from pyib_b200.batch import BatchRun, partition, sweep_cases
 
     build.build_library()
-    if world > 1:
-        raise SystemExit("the batched sweep runs on one GPU")
+    dist = maybe_init_dist(world, local)
     cases = sweep_cases(args.batch_cases, seed=0)
+    parts, loads = partition(cases, world, steps=args.steps)
+    mine = [cases[q] for q in parts[rank]]
     t_setup = time.perf_counter()
-    batch = BatchRun(cases, device=0, precision=args.precision, mixed_tol=args.mixed_tol)
+    batch = BatchRun(mine, device=local if world > 1 else 0, precision=args.precision, mixed_tol=args.mixed_tol)
     batch.tune()
     setup_s = time.perf_counter() - t_setup
     cells = batch.cells
     for _ in range(args.warmup):
         batch.advance(1, concurrent=True)
-    sampler = ClockSampler(0)
-    sampler.start()
-    t_con, st_con = batch.advance(args.steps, concurrent=True)
-    t_seq, st_seq = batch.advance(args.steps, concurrent=False)
-    clocks = sampler.stop()
-    upd = float(sum(cells)) * args.steps
+    barrier(dist)
+    sampler = ClockSampler(local if world > 1 else 0) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    t_con, st_con = batch.advance(args.steps, concurrent=True) if mine else (0.0, {"cg_iterations": 0,
+                                                                               "max_case_iterations": 0})
+    barrier(dist)
+    t_seq, st_seq = batch.advance(args.steps, concurrent=False) if mine else (0.0, {"cg_iterations": 0,
+                                                                                "max_case_iterations": 0})
+    clocks = sampler.stop() if sampler else None
     launches = 0
     timing = (C.c_double * 5)()
     for r in batch.runs:
         r.drv.solver.h.call("pyib_cg_timing", timing, 0)
         launches += int(timing[2])
+    con = aggregate_batch(dist, t_con, t_seq, sum(cells), launches, st_con["cg_iterations"],
+                          st_con["max_case_iterations"])
+    seq = aggregate_batch(dist, t_con, t_seq, sum(cells), 0, st_seq["cg_iterations"],
+                          st_seq["max_case_iterations"])
+    batch.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    upd = con["cells"] * args.steps
     line = {
-        "metric": "batched sweep cell-updates/s", "value": upd / t_con, "unit": "cell-updates/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_con / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": "batched sweep cell-updates/s", "value": upd / con["seconds_concurrent"],
+        "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * con["seconds_concurrent"] / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64" if args.precision == "float64" else "f32+f64", "data": "synthetic",
         "config": {"workload": "batched_sweep", "cases": len(cases), "seed": 0,
-                   "cells_per_diameter_histogram": batch.histogram(), "total_cells": int(sum(cells)),
-                   "levels": 2, "precision": args.precision, "setup_seconds": setup_s,
-                   "l2": "inputs larger than L2"},
-        "concurrent": {"seconds": t_con, **st_con},
-        "one_at_a_time": {"value": upd / t_seq, "seconds": t_seq, **st_seq},
-        "gpu_launches_since_setup": launches,
+                   "cells_per_diameter_histogram": dict(sorted(Counter(c.cells_per_diameter
+                                                                       for c in cases).items())),
+                   "total_cells": int(con["cells"]), "levels": 2, "precision": args.precision,
+                   "setup_seconds": setup_s, "l2": "inputs larger than L2",
+                   "parallelism": f"cases split over {world} GPU(s) by cells x steps",
+                   "cells_per_rank": [int(x // args.steps) for x in loads]},
+        "concurrent": {"seconds": con["seconds_concurrent"], "cg_iterations": int(con["cg_iterations"]),
+                       "max_case_iterations": int(con["max_case_iterations"])},
+        "one_at_a_time": {"value": upd / seq["seconds_sequential"], "seconds": seq["seconds_sequential"],
+                          "cg_iterations": int(seq["cg_iterations"]),
+                          "max_case_iterations": int(seq["max_case_iterations"])},
+        "gpu_launches_since_setup": int(con["launches"]),
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
-    batch.close()
     return 0
 
 

@@ -45,6 +45,37 @@ def sweep_cases(count=64, seed=0, cg_max_iterations=20000):
     return out
 
 
+def case_cost(case, steps=1):
+    """Work of one case: existing cells x steps (every case advances the same
+    number of steps, each step touching every cell).  Level L of the concentric
+    layout is a box of ``2 hw_L n / 2^L`` cells per axis (``n`` cells per
+    diameter), less the finer box it contains."""
+    n = int(case.cells_per_diameter)
+    cells, finer = 0, 0
+    for L, hw in enumerate(case.half_widths_d):
+        side = int(round(2.0 * float(hw) * n / 2 ** L))
+        cells += side ** 3 - (finer // 2) ** 3
+        finer = side
+    return cells * int(steps)
+
+
+def partition(cases, world, steps=1):
+    """Cases split across ``world`` GPUs by cost: longest first, each to the rank with
+    the least work so far (lowest rank on ties).  Deterministic; every case appears
+    once; each rank's list keeps the sweep order."""
+    world = int(world)
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    costs = [case_cost(c, steps) for c in cases]
+    load = [0] * world
+    owner = [0] * len(cases)
+    for q in sorted(range(len(cases)), key=lambda i: (-costs[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[q] = r
+        load[r] += costs[q]
+    return [[q for q in range(len(cases)) if owner[q] == r] for r in range(world)], load
+
+
 class BatchRun:
     """Independent sphere cases on one GPU, stepped concurrently or one at a time."""
 

@@ -59,3 +59,31 @@ def test_reference_arm_other_ranks_exit_without_work(capsys):
 
     assert bench.run_reference(Args, world=2, rank=1) == 0
     assert capsys.readouterr().out == ""
+
+
+def _batch_worker(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    import bench
+    w, r, local = bench.dist_env()
+    dist = bench.maybe_init_dist(w, local, backend="gloo")
+    agg = bench.aggregate_batch(dist, seconds_concurrent=2.0 + rank, seconds_sequential=5.0 - rank,
+                                cells=1000 * (rank + 1), launches=7, cg_iterations=100 + rank,
+                                max_case_iterations=40 + 10 * rank)
+    (Path(out_dir) / f"batch{rank}.json").write_text(json.dumps(agg))
+    dist.destroy_process_group()
+
+
+def test_sharded_sweep_reductions_on_two_gloo_ranks(tmp_path):
+    """The sharded batched sweep's whole-job figures: the slowest rank's times and the
+    summed work, identical on every rank."""
+    world = 2
+    mp.start_processes(_batch_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    res = [json.loads((tmp_path / f"batch{r}.json").read_text()) for r in range(world)]
+    assert res[0] == res[1]
+    a = res[0]
+    assert a["seconds_concurrent"] == 3.0 and a["seconds_sequential"] == 5.0
+    assert a["cells"] == 3000 and a["launches"] == 14
+    assert a["cg_iterations"] == 201 and a["max_case_iterations"] == 50
