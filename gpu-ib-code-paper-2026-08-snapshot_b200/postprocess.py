@@ -70,6 +70,14 @@ def default_handle(device=0):
     return h
 
 
+def close_default_handles():
+    """Release this host thread's default contexts and their workspaces."""
+    handles = getattr(_local, "handles", None) or {}
+    for h in handles.values():
+        h.close()
+    handles.clear()
+
+
 def laplacian_csr(count, first, second, weights):
     """CSR of ``B^T diag(w) B`` (B: the signed face-cell incidence), duplicates summed,
     columns ascending within each row."""

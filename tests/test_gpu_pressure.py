@@ -79,6 +79,19 @@ def test_quadratic_known_answer_128_cubed():
     assert 0 < diag["iterations"] < 10 * c ** 3
 
 
+def test_default_context_is_kept_and_can_be_released():
+    args = n2_inputs()
+    PP.recover_pressure(*args)
+    h = PP.default_handle(0)
+    PP.recover_pressure(*args)
+    assert PP.default_handle(0) is h            # the same context, its workspace kept
+    PP.close_default_handles()
+    assert not h.ptr
+    p, _ = PP.recover_pressure(*args)           # a new one is made on demand
+    assert PP.default_handle(0) is not h
+    assert np.max(np.abs(p - GOLD["n2_pressure"])) <= 1e-9 * np.max(np.abs(GOLD["n2_pressure"]))
+
+
 def test_solver_handle_is_reused_and_errors_are_reported():
     args = n2_inputs()
     h = PP.bare_handle(0)
