@@ -45,7 +45,13 @@ class Operators:
             self._cell_face(lay, NC, NF)
             self.C, self.R = f_curl.result()
             self.AoL = f_aol.result()
-        self.Vd = (sp.diags(self.vol_ci) @ self.D @ sp.diags(self.AoL) @ self.G0).tocsr()
+        # vol * D * diag(AoL) is a row and column scaling of D's entries, in the order
+        # the two diagonal products take (the same bits); then one sparse product
+        D = self.D
+        drow = np.repeat(np.arange(D.shape[0]), np.diff(D.indptr))
+        Dw = sp.csr_matrix(((self.vol_ci[drow] * D.data) * self.AoL[D.indices], D.indices, D.indptr),
+                           shape=D.shape)
+        self.Vd = (Dw @ self.G0).tocsr()
 
     def _cell_face(self, lay, NC, NF):
         """P, I, D, G0 and the face data and entry orders they share."""
@@ -61,8 +67,10 @@ class Operators:
         # that list them as rows of cells x faces and of faces x cells
         rows = np.concatenate([lo[mlo], hi[mhi]])
         cols = np.concatenate([f[mlo], f[mhi]])
-        self.cf = self._pattern(rows, cols, NC)
-        self.fc = self._pattern(cols, rows, NF)
+        with ThreadPoolExecutor(max_workers=2) as pool:      # two independent sorts
+            f_cf = pool.submit(self._pattern, rows, cols, NC)
+            f_fc = pool.submit(self._pattern, cols, rows, NF)
+            self.cf, self.fc = f_cf.result(), f_fc.result()
         self.faces = dict(f=f, lo=lo, hi=hi, mlo=mlo, mhi=mhi, dlo=dlo, dhi=dhi, rows=rows, cols=cols)
         self.P, self.I = [], []
         ccf, cfc = {}, {}
