@@ -18,3 +18,17 @@ def test_reference_arm_prints_its_line():
         assert key in line, key
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_pressure_reference_arm_prints_its_line():
+    """The offline pressure recovery's reference arm: the oracle (scipy cg, the
+    reference's algorithm) on the 64^3 sample, row-iterations/s."""
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload",
+                          "pressure_recovery_128", "--steps", "1", "--warmup", "3"],
+                         capture_output=True, text=True, timeout=600, cwd=str(ROOT))
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "row-iterations/s"
+    assert line["config"]["workload"] == "pressure_recovery_128"
+    assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"]["value"] == line["value"]
