@@ -370,7 +370,22 @@ def diagnostics(rt: CaseRuntime, step, ms_per_step):
     return row
 
 
+def _sync_directory(directory: Path) -> None:
+    """Flush a directory entry (a rename) to disk; best effort, as on filesystems without dir fsync."""
+    try:
+        fd = os.open(directory, os.O_RDONLY)
+    except OSError:
+        return
+    try:
+        os.fsync(fd)
+    except OSError:
+        pass
+    finally:
+        os.close(fd)
+
+
 def _atomic_npz(path: Path, **arrays):
+    """Write, fsync, rename over ``path``, then fsync the directory so the rename survives a crash."""
     tmp = path.with_name(f".{path.stem}.{uuid.uuid4().hex}.tmp.npz")
     try:
         np.savez(tmp, **arrays)
@@ -378,6 +393,7 @@ def _atomic_npz(path: Path, **arrays):
             fh.flush()
             os.fsync(fh.fileno())
         os.replace(tmp, path)
+        _sync_directory(path.parent)
     finally:
         if tmp.exists():
             tmp.unlink()

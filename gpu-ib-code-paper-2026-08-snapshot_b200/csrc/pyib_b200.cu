@@ -1602,6 +1602,7 @@ __global__ void k_ib_segsum(long long tot, long long nc, const int* __restrict__
        t += (long long)gridDim.x * blockDim.x) {
     const int key = keys[t];
     if (t > 0 && keys[t - 1] == key) continue;
+    if (key < 0 || key >= nc) continue;            // rejected contributions (sentinel key nc)
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     for (long long q = t; q < tot && keys[q] == key; ++q) {
       const int src = vals[q];
@@ -3419,12 +3420,31 @@ constexpr long long kNoAllocMaxMarkers = 8192;                      // 1,024,000
 constexpr long long kNoAllocMaxItems = kNoAllocMaxMarkers * 125;
 constexpr size_t kNoAllocSortBytes = 4ull * kNoAllocMaxItems * sizeof(int);   // 16,384,000
 constexpr size_t kNoAllocTempBytes = 1ull << 20;                   // CUB histograms and offsets
-constexpr size_t kNoAllocBytes = kNoAllocSortBytes + kNoAllocTempBytes;
+constexpr size_t kNoAllocStatusBytes = 256;                        // reject counter
+constexpr size_t kNoAllocBytes = kNoAllocSortBytes + kNoAllocTempBytes + kNoAllocStatusBytes;
 constexpr int kNoAllocMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_spread_scratch[kNoAllocBytes];
 static void* g_spread_scratch_ptr[kNoAllocMaxDevices] = {nullptr};
+
+namespace {
+// Keys for the no-allocation spreading: caller-supplied cell ids are checked
+// against [0, ncell).  A bad id gets the sentinel key ncell, which sorts after
+// every valid cell and which k_ib_segsum skips, so it writes nothing; the
+// rejects are counted in a word of the fixed scratch array.
+__global__ void k_noalloc_keys(long long tot, long long ncell, const int* __restrict__ cell, int* keys,
+                               int* vals, unsigned int* rejects) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = cell[t];
+    const bool ok = c >= 0 && (long long)c < ncell;
+    keys[t] = ok ? c : (int)ncell;
+    vals[t] = (int)t;
+    if (!ok) atomicAdd(rejects, 1u);
+  }
+}
+}  // namespace
 
 extern "C" int pyib_spread_noalloc(const int32_t* cell, const double* w, const double* ds3, const double* f,
                                    int32_t nmarkers, int64_t ncell, double* out, void* stream) {
@@ -3447,19 +3467,28 @@ extern "C" int pyib_spread_noalloc(const int32_t* cell, const double* w, const d
   int* vals_a = keys_b + kNoAllocMaxItems;
   int* vals_b = vals_a + kNoAllocMaxItems;
   void* temp = (void*)((unsigned char*)g_spread_scratch_ptr[dev] + kNoAllocSortBytes);
+  unsigned int* rejects =
+      (unsigned int*)((unsigned char*)g_spread_scratch_ptr[dev] + kNoAllocSortBytes + kNoAllocTempBytes);
+  // enough key bits for every valid id and the sentinel ncell (ncell < 2^31)
   int nbits = 1;
-  while (nbits < 31 && (1LL << nbits) < ncell) ++nbits;
+  while (nbits < 31 && (1LL << nbits) <= ncell) ++nbits;
   cub::DoubleBuffer<int> dk(keys_a, keys_b), dv(vals_a, vals_b);
   size_t tb = 0;
   if (cub::DeviceRadixSort::SortPairs((void*)nullptr, tb, dk, dv, (int)tot, 0, nbits, s) != cudaSuccess)
     return PYIB_E_CUDA;
   if (tb > kNoAllocTempBytes) return PYIB_E_ARG;
   if (cudaMemsetAsync(out, 0, 3 * (size_t)ncell * sizeof(double), s) != cudaSuccess) return PYIB_E_CUDA;
-  k_ib_keys<<<grid_for(tot), kThreads, 0, s>>>(tot, cell, w, dk.Current(), dv.Current());
+  // the array keeps the previous call's contents: the reject count starts at zero
+  if (cudaMemsetAsync(rejects, 0, sizeof(unsigned int), s) != cudaSuccess) return PYIB_E_CUDA;
+  k_noalloc_keys<<<grid_for(tot), kThreads, 0, s>>>(tot, ncell, cell, dk.Current(), dv.Current(), rejects);
   if (cudaGetLastError() != cudaSuccess) return PYIB_E_CUDA;
   if (cub::DeviceRadixSort::SortPairs(temp, tb, dk, dv, (int)tot, 0, nbits, s) != cudaSuccess)
     return PYIB_E_CUDA;
   k_ib_segsum<<<grid_for(tot), kThreads, 0, s>>>(tot, ncell, dk.Current(), dv.Current(), w, ds3, f, out);
   if (cudaGetLastError() != cudaSuccess) return PYIB_E_CUDA;
-  return PYIB_OK;
+  // Stream-ordered read of the reject count: the call returns once its work is done.
+  unsigned int bad = 0;
+  if (cudaMemcpyAsync(&bad, rejects, sizeof(bad), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PYIB_E_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return PYIB_E_CUDA;
+  return bad ? PYIB_E_DEVICE : PYIB_OK;
 }

@@ -274,16 +274,20 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
  * All pointers are device pointers: cell/w are the 125*nmarkers stencil cells and
  * weights (PYIB_F_IB_CELL, PYIB_F_IB_W), ds3 the marker volumes, f the marker-major
  * forces, out 3*ncell doubles (component-major, fully overwritten).
- *  - Scratch: one fixed file-scope device array of 17,408,000 bytes, enough for at
+ *  - Scratch: one fixed file-scope device array of 17,408,256 bytes, enough for at
  *    most 8192 markers; larger counts return PYIB_E_ARG.  Every GPU that loads the
  *    library holds this array until the process exits.
+ *  - Cell ids are checked on the device: a contribution whose id lies outside
+ *    [0, ncell) is skipped (nothing is written outside out) and the call returns
+ *    PYIB_E_DEVICE; the valid contributions are still summed into out.
  *  - The first call on a device looks up the array's device address
  *    (cudaGetSymbolAddress) with that device current; make that first call before
  *    any stream capture.
  *  - Calls share the array: calls that overlap on the GPU (different streams, or
  *    threads without ordering) race.  Run them in one stream or serialize them.
- *  - stream is a cudaStream_t (NULL: the legacy default stream).  The call is
- *    asynchronous with respect to the host. */
+ *  - stream is a cudaStream_t (NULL: the legacy default stream).  The call reads
+ *    the count of rejected ids back in stream order, so it returns only after its
+ *    work on that stream has finished. */
 int pyib_spread_noalloc(const int32_t* cell, const double* w, const double* ds3, const double* f,
                         int32_t nmarkers, int64_t ncell, double* out, void* stream);
 

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder by running the unmodified reference.
 
-Run in a container that holds the reference tree (default ``/root/reference``):
+Run where the reference tree is present, named by ``PYIB_REFERENCE_ROOT``:
 
     python tests/golden/make_golden.py
 

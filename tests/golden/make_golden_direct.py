@@ -1,6 +1,6 @@
 """Golden trajectories of the reference's ``direct`` IB force mode, explicit and implicit.
 
-Run in a container that holds the reference tree (default ``/root/reference``):
+Run where the reference tree is present, named by ``PYIB_REFERENCE_ROOT``:
 
     python tests/golden/make_golden_direct.py
 

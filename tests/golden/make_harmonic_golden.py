@@ -1,6 +1,6 @@
 """Golden values for the force harmonic fit, from the reference's own check tool.
 
-Run in a container that holds the reference tree (default ``/root/reference``):
+Run where the reference tree is present, named by ``PYIB_REFERENCE_ROOT``:
 
     python tests/golden/make_harmonic_golden.py
 
@@ -11,12 +11,16 @@ and the reference's coefficients and residual go to ``harmonic_fit.json``.
 import importlib.util
 import json
 import os
+import sys
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("PYIB_REFERENCE_ROOT", "/root/reference"))
+sys.path.insert(0, str(HERE))
+import refharness  # noqa: E402
+
+REF = refharness.reference_root()
 
 spec = importlib.util.spec_from_file_location("check_pressure_validation",
                                               REF / "tools" / "check_pressure_validation.py")

@@ -1,6 +1,6 @@
 """Golden outputs of the reference's offline pressure recovery.
 
-Run in a container that holds the reference tree (default ``/root/reference``):
+Run where the reference tree is present, named by ``PYIB_REFERENCE_ROOT``:
 
     python tests/golden/make_pressure_golden.py
 

@@ -1,8 +1,8 @@
 """Drive the unmodified PyIB reference (CPU NumPy/SciPy path) to produce golden data.
 
-This script runs only in a container that holds the reference source tree at
-``/root/reference``; it is never imported by the product, by ``bench.py`` or by
-the GPU tests.  It builds cases the way ``solver/ib_case.py:build_runtime``
+This script runs only where the reference source tree is present; its location
+comes from the environment variable ``PYIB_REFERENCE_ROOT``.  It is never
+imported by the product, by ``bench.py`` or by the GPU tests.  It builds cases the way ``solver/ib_case.py:build_runtime``
 (lines 633-809) does, but with nested box lists chosen here, because the
 reference's presets do not cover the workloads used by the tests.
 
@@ -18,13 +18,23 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE_ROOT = Path(os.environ.get("PYIB_REFERENCE_ROOT", "/root/reference"))
+def reference_root() -> Path:
+    """The reference source tree, named by the environment variable PYIB_REFERENCE_ROOT."""
+    root = os.environ.get("PYIB_REFERENCE_ROOT")
+    if not root:
+        raise RuntimeError("set PYIB_REFERENCE_ROOT to the PyIB reference source tree "
+                           "(the directory that holds src/pyib)")
+    path = Path(root)
+    if not (path / "src" / "pyib" / "solver").is_dir():
+        raise RuntimeError(f"PYIB_REFERENCE_ROOT={root} does not hold src/pyib/solver")
+    return path
 
 
 def import_reference():
     """Put the reference's modules on sys.path (CPU backend, float64)."""
     if "ib_case" in sys.modules:
         return sys.modules["ib_case"]
+    REFERENCE_ROOT = reference_root()
     stubs = Path(tempfile.mkdtemp(prefix="pyib_stubs_"))
     (stubs / "h5py.py").write_text("")
     (stubs / "meshio.py").write_text("")

@@ -63,3 +63,46 @@ def test_spread_noalloc_rejects_too_many_markers():
     x = torch.zeros(16, dtype=torch.float64, device=dev)
     p = C.c_void_p(x.data_ptr())
     assert lib.pyib_spread_noalloc(p, p, p, p, 8193, 10, p, None) == _lib.E_ARG
+
+
+def test_spread_noalloc_rejects_bad_cell_ids():
+    """Ids outside [0, ncell) are skipped and reported; nothing lands outside out."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5)
+    M, ncell, guard = 4, 300, 64
+    cell = rng.integers(0, ncell, size=M * 125).astype(np.int32)
+    cell[7] = ncell            # one past the end
+    cell[130] = ncell + 1000   # far past the end
+    cell[260] = -3             # negative
+    w = rng.random(M * 125)
+    ds3 = rng.random(M) + 0.5
+    f = rng.standard_normal(3 * M)
+    ok = (cell >= 0) & (cell < ncell)
+    m = np.arange(M * 125) // 125
+    expected = np.zeros(3 * ncell)
+    for d in range(3):
+        contrib = f[3 * m + d] * (w * ds3[m])
+        expected[d * ncell:(d + 1) * ncell] = np.bincount(cell[ok], weights=contrib[ok], minlength=ncell)
+    buf = torch.full((3 * ncell + guard,), float("nan"), dtype=torch.float64, device=dev)
+    t_cell = torch.from_numpy(cell).to(dev)
+    t_w = torch.from_numpy(w).to(dev)
+    t_ds3 = torch.from_numpy(ds3).to(dev)
+    t_f = torch.from_numpy(f).to(dev)
+    for _ in range(2):
+        rc = lib.pyib_spread_noalloc(C.c_void_p(t_cell.data_ptr()), C.c_void_p(t_w.data_ptr()),
+                                     C.c_void_p(t_ds3.data_ptr()), C.c_void_p(t_f.data_ptr()),
+                                     int(M), int(ncell), C.c_void_p(buf.data_ptr()), None)
+        torch.cuda.synchronize(dev)
+        assert rc == _lib.E_DEVICE
+        got = buf.cpu().numpy()
+        assert np.all(np.isnan(got[3 * ncell:]))          # guard after out untouched
+        np.testing.assert_allclose(got[:3 * ncell], expected, rtol=1e-13, atol=1e-15)
+    # a clean call afterwards succeeds: the reject counter starts at zero every call
+    t_cell.clamp_(0, ncell - 1)
+    rc = lib.pyib_spread_noalloc(C.c_void_p(t_cell.data_ptr()), C.c_void_p(t_w.data_ptr()),
+                                 C.c_void_p(t_ds3.data_ptr()), C.c_void_p(t_f.data_ptr()),
+                                 int(M), int(ncell), C.c_void_p(buf.data_ptr()), None)
+    torch.cuda.synchronize(dev)
+    assert rc == _lib.OK
