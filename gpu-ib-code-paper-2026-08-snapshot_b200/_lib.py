@@ -149,6 +149,13 @@ def load():
     return lib
 
 
+def version():
+    """The library's version string (pyib_version)."""
+    buf = C.create_string_buffer(128)
+    load().pyib_version(buf, len(buf))
+    return buf.value.decode()
+
+
 def exported_symbols():
     """Names the header declares that the loaded library resolves."""
     lib = load()

@@ -35,7 +35,8 @@ from .layout import NestedLayout
 from .runner import SphereLoads
 
 SCHEMA_VERSION = 1
-CHECKPOINT_SCHEMA_VERSION = 1
+CHECKPOINT_SCHEMA_VERSION = 3    # the reference's payload (ib_case.py:823-870)
+RESULT_SCHEMA_VERSION = 5        # metadata and field snapshots (ib_case.py:53)
 
 DEFAULT_CONFIG: dict[str, Any] = {
     "schema_version": SCHEMA_VERSION,
@@ -79,6 +80,10 @@ HISTORY_COLUMNS = [
     "force_fluid_x", "force_fluid_y", "force_fluid_z", "body_moment_x", "body_moment_y",
     "body_moment_z", "moment_fluid_x", "moment_fluid_y", "moment_fluid_z",
     "interior_momentum_x", "interior_momentum_y", "interior_momentum_z",
+    "interior_angular_momentum_x", "interior_angular_momentum_y", "interior_angular_momentum_z",
+    "interior_momentum_rate_x", "interior_momentum_rate_y", "interior_momentum_rate_z",
+    "interior_angular_momentum_rate_x", "interior_angular_momentum_rate_y",
+    "interior_angular_momentum_rate_z",
     "interior_indicator_volume", "slip_max", "slip_rms", "speed_max", "cfl", "mass_residual_inf",
     "force_balance_relerr", "ib_force_updates", "helmholtz_iterations",
     "helmholtz_relative_residual", "helmholtz_tolerance_ratio", "milliseconds_per_step",
@@ -271,6 +276,10 @@ class CaseRuntime:
     reference_force: float
     reference_speed: float
     fingerprint: str
+    reference_markers: Any = None
+    compact: Any = None
+    layout_fingerprint: str = ""
+    source_hashes: Any = None
 
 
 def build_runtime(cfg) -> CaseRuntime:
@@ -319,11 +328,14 @@ def build_runtime(cfg) -> CaseRuntime:
     else:
         drv.set_ib(None, markers, ds, np.zeros_like(markers), force_mode=fm)
     loads = SphereLoads(drv, centre, exc, radius, dx, rho, 1.5 * dx)
-    return CaseRuntime(config=cfg, layout=lay, driver=drv, loads=loads, motion=motion, dx=dx,
-                       dt=cfg["time"]["dt"], steps=cfg["time"]["steps"],
-                       inner=cfg["time"]["inner_iterations"],
-                       reference_force=0.5 * rho * uref ** 2 * np.pi * radius ** 2, reference_speed=uref,
-                       fingerprint=config_fingerprint(cfg))
+    rt = CaseRuntime(config=cfg, layout=lay, driver=drv, loads=loads, motion=motion, dx=dx,
+                     dt=cfg["time"]["dt"], steps=cfg["time"]["steps"],
+                     inner=cfg["time"]["inner_iterations"],
+                     reference_force=0.5 * rho * uref ** 2 * np.pi * radius ** 2, reference_speed=uref,
+                     fingerprint=config_fingerprint(cfg), reference_markers=markers,
+                     compact=CompactIds(drv.layout), source_hashes=source_hashes())
+    rt.layout_fingerprint = layout_fingerprint(rt)
+    return rt
 
 
 def sphere_center(rt: CaseRuntime, t):
@@ -334,30 +346,35 @@ def sphere_center(rt: CaseRuntime, t):
 
 
 def diagnostics(rt: CaseRuntime, step, ms_per_step):
-    """A history row (ib_case.py:1129-1224)."""
+    """A history row with the reference's 41 columns (ib_case.py:1129-1224)."""
     drv, load = rt.driver, rt.loads.latest
-    d = np.zeros(4)
+    if load is None:
+        raise RuntimeError("closed-body load correction was not advanced for this step")
     import ctypes as C
     out = (C.c_double * 4)()
     drv.solver.h.call("pyib_diagnostics", out)
-    d[:] = out[:]
+    d = np.asarray(out[:])
     fL = drv.ib_force_L
     lag = (fL * (drv.ib_ds ** 3)[:, None]).sum(axis=0)
     ff = load["force_fluid"]
     den = max(float(np.linalg.norm(lag)), float(np.linalg.norm(ff)), 1e-300)
     balance = float(np.linalg.norm(ff - lag)) / den
     coef = load["body_force"] / rt.reference_force
-    row = {"step": step, "time": drv.time, "Cd": coef[0], "Cy": coef[1], "Cz": coef[2],
+    row = {"step": int(step), "time": float(drv.time), "Cd": float(coef[0]), "Cy": float(coef[1]),
+           "Cz": float(coef[2]),
            "interior_indicator_volume": float(load["indicator_volume"]), "slip_max": d[2], "slip_rms": d[3],
            "speed_max": d[0], "cfl": d[0] * rt.dt / rt.dx, "mass_residual_inf": d[1],
-           "force_balance_relerr": balance, "ib_force_updates": drv.ib_force_updates_last_step,
-           "helmholtz_iterations": drv.helmholtz_iterations_last_step,
-           "helmholtz_relative_residual": drv.helmholtz_relative_residual_last_step,
-           "helmholtz_tolerance_ratio": drv.helmholtz_tolerance_ratio_last_step,
-           "milliseconds_per_step": ms_per_step}
+           "force_balance_relerr": balance, "ib_force_updates": int(drv.ib_force_updates_last_step),
+           "helmholtz_iterations": int(drv.helmholtz_iterations_last_step),
+           "helmholtz_relative_residual": float(drv.helmholtz_relative_residual_last_step),
+           "helmholtz_tolerance_ratio": float(drv.helmholtz_tolerance_ratio_last_step),
+           "milliseconds_per_step": float(ms_per_step)}
     for name, key in (("body_force", "body_force"), ("force_fluid", "force_fluid"),
                       ("body_moment", "body_moment"), ("moment_fluid", "moment_fluid"),
-                      ("interior_momentum", "linear_momentum")):
+                      ("interior_momentum", "linear_momentum"),
+                      ("interior_angular_momentum", "angular_momentum"),
+                      ("interior_momentum_rate", "linear_rate"),
+                      ("interior_angular_momentum_rate", "angular_rate")):
         for a, ax in enumerate("xyz"):
             row[f"{name}_{ax}"] = float(load[key][a])
     vals = np.asarray([float(row[c]) for c in HISTORY_COLUMNS])
@@ -365,31 +382,233 @@ def diagnostics(rt: CaseRuntime, step, ms_per_step):
         raise FloatingPointError(f"non-finite diagnostic at step {step}: {row}")
     if balance > 1e-9 and rt.config["runtime"]["precision"] == "float64":
         raise RuntimeError(f"IB force-spread balance failed at step {step}: {balance:.3e}")
-    if row["ib_force_updates"] != 1:
-        raise RuntimeError(f"IB update-count invariant failed at step {step}")
+    expected = 1 if rt.config["ib"]["force_mode"] == "accumulated_explicit" else rt.inner
+    if row["ib_force_updates"] != expected:
+        raise RuntimeError(f"IB update-count invariant failed at step {step}: "
+                           f"{row['ib_force_updates']} != {expected}")
     return row
 
 
-def _sync_directory(directory: Path) -> None:
-    """Flush a directory entry (a rename) to disk; best effort, as on filesystems without dir fsync."""
-    try:
-        fd = os.open(directory, os.O_RDONLY)
-    except OSError:
-        return
-    try:
-        os.fsync(fd)
-    except OSError:
-        pass
-    finally:
-        os.close(fd)
+# ---------------------------------------------------------------------------
+# run artefacts in the reference's schema
+# ---------------------------------------------------------------------------
+class CompactIds:
+    """Dense layout ids <-> the compact numbering of the exported mesh.
+
+    Checkpoints and field snapshots hold one entry per existing edge / cell /
+    face (the reference's array sizes), in ascending dense id, edge and face
+    values oriented along +axis.
+    """
+
+    def __init__(self, lay):
+        self.lay = lay
+        self.cells = np.nonzero(lay.cell_active)[0]
+        self.faces = np.nonzero(lay.face_exists)[0]
+        self.edges = np.nonzero(lay.edge_exists)[0]
+
+    def edge(self, v):
+        return np.asarray(v, dtype=np.float64)[self.edges]
+
+    def edge_dense(self, v):
+        out = np.zeros(self.lay.NE)
+        out[self.edges] = v
+        return out
+
+    def cell3(self, v3):
+        return np.ascontiguousarray(np.asarray(v3, dtype=np.float64)[:, self.cells].T)
+
+    def cell3_dense(self, v):
+        out = np.zeros((3, self.lay.NC))
+        out[:, self.cells] = np.asarray(v, dtype=np.float64).T
+        return out
 
 
-def _atomic_npz(path: Path, **arrays):
-    """Write, fsync, rename over ``path``, then fsync the directory so the rename survives a crash."""
-    tmp = path.with_name(f".{path.stem}.{uuid.uuid4().hex}.tmp.npz")
+_SOURCE_FILES = ("case.py", "driver.py", "device.py", "layout.py", "operators.py", "templates.py",
+                 "runner.py", "cases.py", "_lib.py", "csrc/pyib_b200.cu")
+
+
+def source_hashes() -> dict:
+    """sha256 of the numerical sources of this path (ib_case.py:474-487 does the same for its own)."""
+    here = Path(__file__).resolve().parent
+    return {name: hashlib.sha256((here / name).read_bytes()).hexdigest() for name in _SOURCE_FILES}
+
+
+def layout_fingerprint(rt: CaseRuntime) -> str:
+    """sha256 of the exported mesh description and the Lagrangian quadrature (ib_case.py:490-510)."""
+    desc, _ = rt.driver.reference_maps()
+    dg = hashlib.sha256()
+    for name in ("nodes", "F2C", "F2E", "E2N", "link_fe_insert", "bc_edge", "bc_face", "index_cell",
+                 "pos_ref"):
+        a = np.ascontiguousarray(np.asarray(desc[name]))
+        dg.update(name.encode() + b"\0" + a.dtype.str.encode() + b"\0" + json.dumps(a.shape).encode() + b"\0")
+        dg.update(a.tobytes())
+    dg.update(np.float64(desc["dx"]).tobytes())
+    for name, value in (("markers", rt.reference_markers), ("marker_widths", rt.driver.ib_ds)):
+        a = np.ascontiguousarray(np.asarray(value, dtype=np.float64))
+        dg.update(name.encode() + b"\0" + json.dumps(a.shape).encode() + b"\0")
+        dg.update(a.tobytes())
+    return dg.hexdigest()
+
+
+def mesh_summary(rt: CaseRuntime) -> dict:
+    """The metadata ``mesh`` block (ib_case.py:640-688): kind, counts, level geometry."""
+    cfg, lay = rt.config, rt.layout
+    desc, _ = rt.driver.reference_maps()
+    mesh = cfg["mesh"]
+    out = {"kind": mesh["kind"], "cells": int(lay.cell_active.sum()), "faces": int(lay.face_exists.sum()),
+           "edges": int(lay.edge_exists.sum()), "nodes": int(desc["nodes"].shape[0]),
+           "markers": int(rt.reference_markers.shape[0])}
+    if mesh["kind"] == "uniform_box":
+        out.update(dx=float(mesh["dx"]), bounds=[list(map(float, b)) for b in mesh["bounds"]])
+    else:
+        D = 2.0 * float(cfg["ib"]["radius"])
+        per = [int(np.count_nonzero(lay.cell_active & (lay.cell_level == L))) for L in range(lay.N)]
+        out.update(D_over_dx=int(mesh["cells_per_diameter"]), diameter=D, dx_fine=float(rt.dx),
+                   layer_cells=per, total_cells=int(sum(per)),
+                   layer_spacing_D=[float(lv.h / D) for lv in lay.levels],
+                   layer_bounds_D=[[float(lv.lo[a] / D) if s == 0 else float(lv.hi[a] / D)
+                                    for a in range(3) for s in (0, 1)] for lv in lay.levels])
+    return out
+
+
+def _checkpoint_payload(rt: CaseRuntime, run_id, step, s, s_old) -> dict:
+    """The schema-3 checkpoint payload (ib_case.py:823-870); arrays in compact order."""
+    drv = rt.driver
+    st = drv.ib_state_dict()
+    if st is None:
+        raise RuntimeError("cannot checkpoint an IB case before Driver.set_ib")
+    load = rt.loads.latest
+    if load is None or rt.loads.current is None:
+        raise RuntimeError("cannot checkpoint before closed-body load bookkeeping")
+    cid = rt.compact
+    return {
+        "checkpoint_schema": np.int64(CHECKPOINT_SCHEMA_VERSION),
+        "update_phase": np.str_("post_step"),
+        "run_id": np.str_(run_id),
+        "config_fingerprint": np.str_(rt.fingerprint),
+        "layout_fingerprint": np.str_(rt.layout_fingerprint),
+        "step": np.int64(step),
+        "physical_time": np.float64(drv.time),
+        "dt": np.float64(rt.dt),
+        "previous_dt": np.float64(rt.dt),
+        "precision": np.str_(rt.config["runtime"]["precision"]),
+        "device": np.str_("b200"),
+        "source_hashes_json": np.str_(json.dumps(rt.source_hashes, sort_keys=True, separators=(",", ":"))),
+        "s": cid.edge(s),
+        "s_old": cid.edge(s_old),
+        "markers": np.asarray(drv.ib_markers, dtype=np.float64),
+        "marker_velocity": np.asarray(drv.ib_vel, dtype=np.float64),
+        "ib_force_mode": np.str_(rt.config["ib"]["force_mode"]),
+        "ib_force_E": cid.cell3(st["force_E"]),
+        "ib_force_L": np.asarray(st["force_L"], dtype=np.float64),
+        "ib_force_update_count": np.int64(st["force_update_count"]),
+        "force_fluid": np.asarray(load["force_fluid"], dtype=np.float64),
+        "moment_fluid": np.asarray(load["moment_fluid"], dtype=np.float64),
+        "body_force": np.asarray(load["body_force"], dtype=np.float64),
+        "body_moment": np.asarray(load["body_moment"], dtype=np.float64),
+        "interior_momentum": np.asarray(load["linear_momentum"], dtype=np.float64),
+        "interior_angular_momentum": np.asarray(load["angular_momentum"], dtype=np.float64),
+        "interior_indicator_volume": np.float64(load["indicator_volume"]),
+        "interior_momentum_rate": np.asarray(load["linear_rate"], dtype=np.float64),
+        "interior_angular_momentum_rate": np.asarray(load["angular_rate"], dtype=np.float64),
+    }
+
+
+def save_checkpoint(path: Path, rt: CaseRuntime, run_id, step, s, s_old):
+    _atomic_npz(path, **_checkpoint_payload(rt, run_id, step, s, s_old))
+
+
+def save_field_snapshot(path: Path, rt: CaseRuntime, run_id, step, s, s_old, vc):
+    """One self-contained field for the offline pressure recovery (ib_case.py:873-911)."""
+    drv, lay, cid = rt.driver, rt.layout, rt.compact
+    if drv.last_step_dt != rt.dt:
+        raise RuntimeError("no current-step momentum residual for pressure recovery")
+    desc, _ = drv.reference_maps()
+    payload = _checkpoint_payload(rt, run_id, step, s, s_old)
+    for name in ("checkpoint_schema", "update_phase", "physical_time", "previous_dt"):
+        payload.pop(name)
+    payload.update(
+        result_schema=np.int64(RESULT_SCHEMA_VERSION),
+        time=np.float64(drv.time),
+        vc=cid.cell3(np.asarray(vc)[:, :lay.NC]),
+        cpos=np.ascontiguousarray(lay.cpos[cid.cells]),
+        cell_volume=np.ascontiguousarray(lay.cell_vol[cid.cells]),
+        marker_volume_weight=np.asarray(drv.ib_ds, dtype=np.float64) ** 3,
+        momentum_residual=cid.cell3(drv.last_momentum_residual),
+        helmholtz_relative_residual=np.float64(drv.helmholtz_relative_residual_last_step),
+        helmholtz_tolerance_ratio=np.float64(drv.helmholtz_tolerance_ratio_last_step),
+        face_cells=np.asarray(desc["F2C"], dtype=np.int64),
+        face_area=np.ascontiguousarray(lay.face_Af[cid.faces]),
+        index_cell=np.asarray(desc["index_cell"], dtype=np.int64),
+        lattice_origin=np.asarray(desc["pos_ref"], dtype=np.float64),
+        lattice_spacing=np.float64(rt.dx),
+        sphere_center=np.asarray(sphere_center(rt, drv.time), dtype=np.float64),
+        sphere_radius=np.float64(rt.config["ib"]["radius"]),
+        density=np.float64(drv.rou),
+        kinematic_viscosity=np.float64(drv.visc / drv.rou),
+    )
+    _atomic_npz(path, **payload)
+
+
+def _str(d, k):
+    return str(d[k].item() if hasattr(d[k], "item") else d[k])
+
+
+def load_checkpoint(path: Path, rt: CaseRuntime):
+    """Validate and restore a schema-3 checkpoint (ib_case.py:914-1121, the checks this path has)."""
     try:
-        np.savez(tmp, **arrays)
-        with tmp.open("r+b") as fh:
+        d = np.load(path, allow_pickle=False)
+    except (OSError, ValueError) as exc:
+        raise CaseConfigError(f"cannot read checkpoint {path}: {exc}") from exc
+    with d:
+        if "checkpoint_schema" not in d.files or int(d["checkpoint_schema"]) != CHECKPOINT_SCHEMA_VERSION:
+            raise CaseConfigError("unsupported checkpoint schema")
+        if _str(d, "update_phase") != "post_step":
+            raise CaseConfigError("checkpoint is not a post-step state")
+        if _str(d, "config_fingerprint") != rt.fingerprint:
+            raise CaseConfigError("checkpoint was written for a different configuration")
+        if _str(d, "layout_fingerprint") != rt.layout_fingerprint:
+            raise CaseConfigError("checkpoint layout fingerprint does not match the configured mesh")
+        if _str(d, "device") != "b200" or _str(d, "precision") != rt.config["runtime"]["precision"]:
+            raise CaseConfigError("checkpoint device/precision differ from the configuration")
+        if float(d["dt"]) != rt.dt or float(d["previous_dt"]) != rt.dt:
+            raise CaseConfigError("checkpoint dt differs from the configuration")
+        if json.loads(_str(d, "source_hashes_json")) != rt.source_hashes:
+            raise CaseConfigError("checkpoint was written by different numerical source files")
+        cid = rt.compact
+        s, s_old = np.asarray(d["s"]), np.asarray(d["s_old"])
+        if s.shape != (cid.edges.size,) or s_old.shape != (cid.edges.size,):
+            raise CaseConfigError("checkpoint layout does not match the configuration")
+        arrays = {k: np.asarray(d[k]) for k in d.files if d[k].dtype.kind == "f"}
+        for k, arr in arrays.items():
+            if not np.all(np.isfinite(arr)):
+                raise CaseConfigError(f"checkpoint field {k} holds non-finite values")
+        step = int(d["step"])
+        drv = rt.driver
+        if abs(float(d["physical_time"]) - step * rt.dt) > 1e-12 * max(1.0, step * rt.dt):
+            raise CaseConfigError("checkpoint time is not anchored to its step")
+        drv.time = step * rt.dt
+        if rt.motion is not None:
+            mk, v = rt.motion(drv.time)
+            drv.set_ib(drv.ib, mk, drv.ib_ds, v, force_mode=drv.ib_force_mode)
+        if not np.array_equal(np.asarray(d["markers"]), np.asarray(drv.ib_markers)):
+            raise CaseConfigError("checkpoint markers disagree with the prescribed motion")
+        fE = cid.cell3_dense(d["ib_force_E"])
+        mode = "replacement" if _str(d, "ib_force_mode") == "direct" else "accumulated_explicit"
+        drv.load_ib_state_dict({"force_mode": mode, "force_E": fE, "force_L": np.asarray(d["ib_force_L"]),
+                                "force_update_count": int(d["ib_force_update_count"])})
+        cur = np.concatenate([d["force_fluid"], d["moment_fluid"], d["interior_momentum"],
+                              d["interior_angular_momentum"], [float(d["interior_indicator_volume"])]])
+        rt.loads.current = cur
+        run_id = _str(d, "run_id")
+        return step, cid.edge_dense(s), cid.edge_dense(s_old), run_id
+
+
+def _atomic_json(path: Path, payload: dict):
+    tmp = path.with_name(f".{path.name}.{uuid.uuid4().hex}.tmp")
+    try:
+        with tmp.open("x", encoding="utf-8") as fh:
+            fh.write(json.dumps(payload, indent=2, allow_nan=False) + "\n")
             fh.flush()
             os.fsync(fh.fileno())
         os.replace(tmp, path)
@@ -399,77 +618,126 @@ def _atomic_npz(path: Path, **arrays):
             tmp.unlink()
 
 
-def save_checkpoint(path: Path, rt: CaseRuntime, step, s, s_old):
-    drv = rt.driver
-    st = drv.ib_state_dict()
-    cur = rt.loads.current
-    _atomic_npz(path, schema=np.int64(CHECKPOINT_SCHEMA_VERSION), fingerprint=np.bytes_(rt.fingerprint),
-                step=np.int64(step), time=np.float64(drv.time), s=np.asarray(s), s_old=np.asarray(s_old),
-                force_E=st["force_E"], force_L=st["force_L"], force_mode=np.bytes_(st["force_mode"]),
-                force_update_count=np.int64(st["force_update_count"]), loads=np.asarray(cur),
-                device=np.bytes_("b200"), precision=np.bytes_(rt.config["runtime"]["precision"]))
+def _metadata(rt: CaseRuntime, run_id, outdir: Path, start_step, resumed_from):
+    """metadata.json with the reference's keys (ib_case.py:1331-1366); backend ``b200/cuda``."""
+    import platform
+    from datetime import datetime, timezone
+    from . import _lib
+    return {
+        "result_schema": RESULT_SCHEMA_VERSION,
+        "run_id": run_id,
+        "created_utc": datetime.now(timezone.utc).isoformat(),
+        "case_name": rt.config["name"],
+        "case_kind": rt.config["case"]["kind"],
+        "backend": "b200/cuda",
+        "precision": rt.config["runtime"]["precision"],
+        "python": platform.python_version(),
+        "array_backend_version": _lib.version(),
+        "config_fingerprint": rt.fingerprint,
+        "layout_fingerprint": rt.layout_fingerprint,
+        "config": rt.config,
+        "mesh": mesh_summary(rt),
+        "dt": rt.dt,
+        "target_steps": rt.steps,
+        "start_step": start_step,
+        "resumed_from": str(Path(resumed_from).resolve()) if resumed_from else None,
+        "output_directory": str(outdir.resolve()),
+        "source_sha256": rt.source_hashes,
+        "closed_body_load": {
+            "method": "Uhlmann interior-fluid momentum correction",
+            "force": "-force_fluid + backward_difference(interior_momentum)",
+            "moment": "-moment_fluid + backward_difference(interior_angular_momentum)",
+            "indicator": "analytic sphere with one-cell linear smoothing",
+            "moment_origin": [0.0, 0.0, 0.0],
+        },
+    }
 
 
-def load_checkpoint(path: Path, rt: CaseRuntime):
-    with np.load(path) as d:
-        if int(d["schema"]) != CHECKPOINT_SCHEMA_VERSION:
-            raise CaseConfigError("unsupported checkpoint schema")
-        if bytes(d["fingerprint"]).decode() != rt.fingerprint:
-            raise CaseConfigError("checkpoint was written for a different configuration")
-        lay = rt.layout
-        s, s_old = np.asarray(d["s"]), np.asarray(d["s_old"])
-        if s.shape != (lay.NE,) or s_old.shape != (lay.NE,):
-            raise CaseConfigError("checkpoint layout does not match the configuration")
-        for arr in (s, s_old, d["force_E"], d["force_L"], d["loads"]):
-            if not np.all(np.isfinite(arr)):
-                raise CaseConfigError("checkpoint holds non-finite values")
-        step = int(d["step"])
-        drv = rt.driver
-        drv.time = step * rt.dt
-        drv.load_ib_state_dict({"force_mode": bytes(d["force_mode"]).decode(), "force_E": d["force_E"],
-                                "force_L": d["force_L"], "force_update_count": int(d["force_update_count"])})
-        rt.loads.current = np.asarray(d["loads"])
-        if rt.motion is not None:
-            mk, v = rt.motion(drv.time)
-            drv.set_ib(drv.ib, mk, drv.ib_ds, v, force_mode=drv.ib_force_mode)
-    return step, s, s_old
+def _archive(outdir: Path, paths):
+    """Move earlier artefacts aside instead of deleting them (ib_case.py:_archive_known_outputs)."""
+    present = [p for p in paths if p.exists()]
+    if not present:
+        return None
+    dest = outdir / "archive" / f"{time.strftime('%Y%m%dT%H%M%S')}-{uuid.uuid4().hex[:8]}"
+    dest.mkdir(parents=True)
+    for p in present:
+        os.replace(p, dest / p.name)
+    _sync_directory(outdir)
+    return dest
+
+
+def _history_prefix(path: Path, start_step: int):
+    """Rows up to the checkpoint step, checked for the reference's columns (ib_case.py:1227-1291)."""
+    if not path.exists():
+        raise CaseConfigError("resume needs the run's history.csv")
+    with path.open(newline="") as fh:
+        reader = csv.DictReader(fh)
+        if reader.fieldnames != HISTORY_COLUMNS:
+            raise CaseConfigError("history.csv does not have the expected columns")
+        rows = [r for r in reader if int(float(r["step"])) <= start_step]
+    if not rows or int(float(rows[-1]["step"])) != start_step:
+        raise CaseConfigError("history.csv has no row for the checkpoint step")
+    return rows
 
 
 def run_case(config, outdir, *, resume=False, overwrite=False, quiet=False):
-    """Run one case; returns a summary dict (ib_case.py:1413-1648)."""
+    """Run one case and write the reference's artefacts (ib_case.py:1413-1648).
+
+    Artefacts: ``history.csv`` (41 columns), ``metadata.json``, ``checkpoint.npz``
+    (schema 3), ``snapshots/field_*.npz`` every ``output.field_every`` steps and
+    ``final_field.npz``.  ``resume=True`` continues from ``checkpoint.npz``.
+    """
+    setup0 = time.perf_counter()
     rt = build_runtime(config)
     out = Path(outdir)
     out.mkdir(parents=True, exist_ok=True)
-    hist_path, ckpt = out / "history.csv", out / "checkpoint.npz"
-    if not resume and not overwrite and (hist_path.exists() or ckpt.exists()):
+    hist_path, ckpt, meta_path = out / "history.csv", out / "checkpoint.npz", out / "metadata.json"
+    final_path, snap_dir = out / "final_field.npz", out / "snapshots"
+    known = (hist_path, ckpt, meta_path, final_path, snap_dir)
+    if not resume and not overwrite and any(p.exists() for p in known):
         raise FileExistsError(f"{out} already contains run artifacts; pass overwrite=True or resume=True")
     drv = rt.driver
-    t_setup = time.perf_counter()
+    previous = None
     if resume:
-        start, s, s_old = load_checkpoint(ckpt, rt)
-        rows = []
-        if hist_path.exists():
-            with hist_path.open() as fh:
-                rows = [r for r in csv.DictReader(fh) if int(float(r["step"])) <= start]
+        start, s, s_old, run_id = load_checkpoint(ckpt, rt)
+        if start >= rt.steps:
+            raise CaseConfigError(f"target steps ({rt.steps}) must exceed checkpoint step ({start})")
+        rows = _history_prefix(hist_path, start)
+        if meta_path.exists():
+            previous = json.loads(meta_path.read_text())
+            if previous.get("run_id") != run_id:
+                raise CaseConfigError("metadata.json belongs to a different run")
+        _archive(out, (final_path,))
+        stale = [p for p in snap_dir.glob("field_*.npz") if p.stem[6:].isdigit() and int(p.stem[6:]) > start]
+        _archive(out, stale)
+        s, _, _ = drv.calc_vel(s)
     else:
         start = 0
         s = drv.initial_stream_function(rt.config["physics"]["inflow_speed"])
         s, _, _ = drv.calc_vel(s)
         s_old = np.asarray(s).copy()
         rt.loads.initialize(sphere_center(rt, 0.0))
+        run_id = str(uuid.uuid4())
         rows = []
-    if start >= rt.steps:
-        raise CaseConfigError(f"target steps ({rt.steps}) must exceed checkpoint step ({start})")
-    meta = {"name": rt.config["name"], "device": "b200", "precision": rt.config["runtime"]["precision"],
-            "fingerprint": rt.fingerprint, "cells": int(rt.layout.cell_active.sum()),
-            "edges": int(rt.layout.edge_exists.sum()), "markers": int(drv.ib_markers.shape[0]),
-            "setup_seconds": time.perf_counter() - t_setup, "start_step": start}
-    (out / "metadata.json").write_text(json.dumps(meta, indent=2) + "\n")
+        if overwrite:
+            _archive(out, known)
+    meta = _metadata(rt, run_id, out, start, ckpt if resume else None)
+    if previous is not None:
+        from datetime import datetime, timezone
+        meta["created_utc"] = previous["created_utc"]
+        meta["resume_count"] = int(previous.get("resume_count", 0)) + 1
+        meta["last_resume_utc"] = datetime.now(timezone.utc).isoformat()
+    else:
+        meta["resume_count"] = 0
+    meta["setup_seconds"] = time.perf_counter() - setup0
+    _atomic_json(meta_path, meta)
     fh = hist_path.open("w", newline="")
     writer = csv.DictWriter(fh, fieldnames=HISTORY_COLUMNS)
     writer.writeheader()
     for r in rows:
         writer.writerow(r)
+    fh.flush()
+    os.fsync(fh.fileno())
     stop = {"flag": False}
     old = {}
     for nm in ("SIGTERM", "SIGINT", "SIGUSR1"):
@@ -483,6 +751,20 @@ def run_case(config, outdir, *, resume=False, overwrite=False, quiet=False):
     o = rt.config["output"]
     done = start
     t0, s0 = time.perf_counter(), start
+    vc = None
+
+    def sample_row(step):
+        nonlocal t0, s0
+        now = time.perf_counter()
+        row = diagnostics(rt, step, (now - t0) * 1000.0 / max(step - s0, 1))
+        t0, s0 = now, step
+        writer.writerow(row)
+        fh.flush()
+        if not quiet:
+            print(f"step={step:6d} t={row['time']:9.5f} Cd={row['Cd']:10.5f} slip={row['slip_max']:.4e} "
+                  f"mass={row['mass_residual_inf']:.2e} CG={row['helmholtz_iterations']:5d} "
+                  f"{row['milliseconds_per_step']:8.1f} ms/step", flush=True)
+
     try:
         for step in range(start + 1, rt.steps + 1):
             drv.time = (step - 1) * rt.dt
@@ -490,22 +772,27 @@ def run_case(config, outdir, *, resume=False, overwrite=False, quiet=False):
             drv.time = step * rt.dt
             rt.loads.advance(sphere_center(rt, drv.time), rt.dt)
             done = step
-            due = (o["checkpoint_every"] and step % o["checkpoint_every"] == 0) or step == rt.steps \
-                or stop["flag"]
-            if step <= 3 or step % o["sample_every"] == 0 or due:
-                now = time.perf_counter()
-                row = diagnostics(rt, step, (now - t0) * 1000.0 / max(step - s0, 1))
-                t0, s0 = now, step
-                writer.writerow(row)
-                fh.flush()
-                if not quiet:
-                    print(f"step={step:6d} t={row['time']:9.5f} Cd={row['Cd']:10.5f} "
-                          f"CG={row['helmholtz_iterations']:5d} {row['milliseconds_per_step']:8.1f} ms/step",
-                          flush=True)
+            ce = int(o["checkpoint_every"])
+            due = bool((ce and step % ce == 0) or step == rt.steps or stop["flag"])
+            sample = step <= 3 or step % o["sample_every"] == 0 or step == rt.steps or due
+            if sample:
+                sample_row(step)
             if due:
+                # the history row must be durable before the checkpoint that names it
                 fh.flush()
                 os.fsync(fh.fileno())
-                save_checkpoint(ckpt, rt, step, s, s_old)
+                save_checkpoint(ckpt, rt, run_id, step, s, s_old)
+            fe = int(o["field_every"])
+            if fe and step >= int(o["field_start_step"]) and step % fe == 0 and \
+                    not (step == rt.steps and o["save_field"]):
+                snap_dir.mkdir(exist_ok=True)
+                save_field_snapshot(snap_dir / f"field_{step:09d}.npz", rt, run_id, step, s, s_old, vc)
+            if stop["flag"] and not due:
+                if not sample:
+                    sample_row(step)
+                fh.flush()
+                os.fsync(fh.fileno())
+                save_checkpoint(ckpt, rt, run_id, step, s, s_old)
             if stop["flag"]:
                 break
     finally:
@@ -515,9 +802,14 @@ def run_case(config, outdir, *, resume=False, overwrite=False, quiet=False):
                 signal.signal(sig, h)
             except (OSError, ValueError):
                 pass
-    meta.update(completed_step=done, complete=done == rt.steps)
-    (out / "metadata.json").write_text(json.dumps(meta, indent=2) + "\n")
-    return {"completed_step": done, "stopped": done != rt.steps, "body_force": rt.loads.latest["body_force"]}
+    if done == rt.steps and o["save_field"] and vc is not None:
+        save_field_snapshot(final_path, rt, run_id, done, s, s_old, vc)
+    from datetime import datetime, timezone
+    meta.update(completed_utc=datetime.now(timezone.utc).isoformat(), completed_step=done,
+                complete=done == rt.steps)
+    _atomic_json(meta_path, meta)
+    return {"completed_step": done, "stopped": done != rt.steps, "run_id": run_id,
+            "body_force": rt.loads.latest["body_force"] if rt.loads.latest is not None else None}
 
 
 def main(argv=None):

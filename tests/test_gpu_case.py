@@ -35,7 +35,8 @@ def test_run_and_resume_reproduce_the_straight_run(tmp_path):
     assert resumed["completed_step"] == 6
     a = np.load(tmp_path / "a" / "checkpoint.npz")
     b = np.load(tmp_path / "b" / "checkpoint.npz")
-    for k in ("s", "s_old", "force_E", "force_L", "loads"):
+    for k in ("s", "s_old", "ib_force_E", "ib_force_L", "force_fluid", "interior_momentum",
+              "interior_angular_momentum", "body_force"):
         assert np.array_equal(a[k], b[k]), k                 # deterministic kernels: bit-identical
     assert np.array_equal(straight["body_force"], resumed["body_force"])
 
