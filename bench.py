@@ -161,60 +161,127 @@ def barrier(dist):
 # ---------------------------------------------------------------------------
 # CPU reference arm: the oracle (NumPy restatement of the reference CPU path)
 # ---------------------------------------------------------------------------
-def reference_sample(case, iters_per_step, cg_iters=6, threads=None):
-    """Time the oracle on a bounded sample and scale to one step of ``case``.
+def cpu_info():
+    """Host threads this process may use and the CPU model name (/proc/cpuinfo)."""
+    model = "unknown"
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return cores_used(), model
 
-    The sample runs the oracle's stencils (calc_vel, conv_diff, rot(integr_c2f))
-    and ``cg_iters`` PCG iterations (matrix-free flow_mat + vector updates, the
-    reference's CPU algorithm) on the same three-level oscillating-sphere
-    layout at D = 8 cells (90,112 cells; the full D = 32 layout needs several
-    minutes and ~20 GB just to assemble the oracle's geometry).  Costs are
-    scaled to the full layout by edge count (per-edge work is the same) and
-    to one step by the CG iteration count per step of the full case.
+
+def committed_iterations_per_step(case):
+    """CG iterations per step of ``case`` from the committed bench record, if any."""
+    f = ROOT / "profiles" / f"bench_{case.name.split('_')[0]}_float64.json"
+    try:
+        return float(json.loads(f.read_text().splitlines()[0])["config"]["cg_iterations_per_step"]), f.name
+    except (OSError, ValueError, KeyError, IndexError):
+        return D32_ITERS_PER_STEP, "bench.D32_ITERS_PER_STEP"
+
+
+class ReferenceSample:
+    """The oracle -- the reference's CPU algorithm restated in NumPy -- on the FULL layout.
+
+    Setup builds the workload's own mesh description (the layout's export in the
+    reference's conventions) and the oracle driver on it: the unstructured
+    incidence operators with ``bincount`` reductions of ``ib_core_np.py``.  Then:
+
+    * ``time_ops`` times one ``calc_vel``, one ``conv_diff`` and one
+      ``rot(integr_c2f(.))`` and weights them by their calls per step in
+      ``Driver.step`` (6, 5 and 4, ``ib_driver_np.py:412-532``);
+    * ``time_iterations`` runs real PCG iterations of ``helm_solve``'s recurrence
+      (``ib_driver_np.py:386-403``: w = A p masked, alpha = eta / p.w, x and r
+      updates, z = prec r, beta = eta' / eta) on a residual of the step's form,
+      once with the default BLAS threads and once limited to one thread.
+
+    A full step needs its CG iteration count of such iterations (about 19,400 at
+    D = 32: 37 CPU hours), so steps/s is the measured per-operation times times
+    that count: an extrapolation of measured full-size work, labelled as such.
     """
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyib_oracle as O
-    from pyib_b200.cases import SphereCase
-    small = SphereCase(name="sample", cells_per_diameter=8, half_widths_d=case.half_widths_d,
-                       reynolds=case.reynolds, amplitude_d=case.amplitude_d)
-    lay = small.layout().build()
-    desc, _ = lay.export_mesh()
-    m = O.MeshDesc(**desc)
-    drv = O.OracleDriver(m, small.viscosity, small.density, cavity=True)
-    ne_small = m.E2N.shape[0]
-    ne_full = full_edge_count(case)
-    rng = np.random.default_rng(0)
-    s = rng.standard_normal(ne_small) * 1e-3
-    dt = small.time_step
-    t0 = time.perf_counter()
-    for _ in range(6):
-        s2, U, vc = drv.calc_vel(s)
-    for _ in range(5):
+
+    def __init__(self, case):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyib_oracle as O
+        t0 = time.perf_counter()
+        lay = case.layout().build()
+        desc, _ = lay.export_mesh()
+        self.m = O.MeshDesc(**desc)
+        self.drv = O.OracleDriver(self.m, case.viscosity, case.density, cavity=case.cavity)
+        self.setup_s = time.perf_counter() - t0
+        self.dt = case.time_step
+        self.ne = self.m.E2N.shape[0]
+        self.nc = self.m.ncell
+        rng = np.random.default_rng(0)
+        self.s = rng.standard_normal(self.ne) * 1e-3
+        drv = self.drv
+        _, _, vc = drv.calc_vel(self.s)
+        res = drv.g.rot(drv.g.integr_c2f(vc[:self.nc] * 0.01))
+        self.r = np.where(drv.dir_mask, 0.0, res)
+        self.x = self.s.copy()
+        self.p = self.r * drv.prec
+        self.eta = float(self.p.dot(self.r))
+
+    def time_ops(self):
+        drv = self.drv
+        t0 = time.perf_counter()
+        _, U, vc = drv.calc_vel(self.s)
+        t1 = time.perf_counter()
         drv.conv_diff(U, vc)
-    for _ in range(4):
-        drv.g.rot(drv.g.integr_c2f(vc[:m.ncell]))
-    t_stencil = time.perf_counter() - t0
-    p = rng.standard_normal(ne_small)
-    r = rng.standard_normal(ne_small)
-    x = np.zeros(ne_small)
-    t0 = time.perf_counter()
-    for _ in range(cg_iters):
-        w = drv.apply(p, dt)
+        t2 = time.perf_counter()
+        drv.g.rot(drv.g.integr_c2f(vc[:self.nc]))
+        t3 = time.perf_counter()
+        self.ops = {"calc_vel": t1 - t0, "conv_diff": t2 - t1, "rot_integr": t3 - t2}
+        return 6 * (t1 - t0) + 5 * (t2 - t1) + 4 * (t3 - t2)
+
+    def iteration(self):
+        drv = self.drv
+        w = drv.apply(self.p, self.dt)
         w[drv.dir_mask] = 0.0
-        a = 1e-3 / max(p.dot(w), 1e-300)
-        x += a * p
-        r -= a * w
-        z = r * drv.prec
-        e = z.dot(r)
-        p = z + 0.5 * p
-    t_iter = (time.perf_counter() - t0) / cg_iters
-    scale = ne_full / ne_small
-    t_step = scale * (t_stencil + iters_per_step * t_iter)
-    sample = (f"oracle on the same 3-level layout at D=8 ({m.ncell} cells, {ne_small} edges): "
-              f"6 calc_vel + 5 conv_diff + 4 rot(integr) = {t_stencil:.2f}s and {cg_iters} PCG "
-              f"iterations at {t_iter*1e3:.1f} ms each; scaled x{scale:.1f} by edges and to "
-              f"{iters_per_step:.0f} CG iterations per step")
-    return 1.0 / t_step, sample
+        den = self.p.dot(w)
+        alf = self.eta / (den if den != 0.0 else np.inf)
+        self.x += alf * self.p
+        self.r -= alf * w
+        z = self.r * drv.prec
+        eta_new = float(z.dot(self.r))
+        beta = eta_new / (self.eta if self.eta != 0.0 else np.inf)
+        self.p = z + beta * self.p
+        self.eta = eta_new
+
+    def time_iterations(self, n, single_thread=False):
+        from contextlib import nullcontext
+        ctx = nullcontext()
+        if single_thread:
+            from threadpoolctl import threadpool_limits
+            ctx = threadpool_limits(limits=1)
+        with ctx:
+            t0 = time.perf_counter()
+            for _ in range(n):
+                self.iteration()
+            return (time.perf_counter() - t0) / n
+
+
+def reference_sample(case, iters_per_step, iters_source, sample=None, n_iter=1):
+    """One bounded sample of the reference's step at full size; returns (steps/s, details)."""
+    rs = sample if sample is not None else ReferenceSample(case)
+    t_ops = rs.time_ops()
+    t_it = rs.time_iterations(n_iter)
+    t_it1 = rs.time_iterations(n_iter, single_thread=True)
+    cores, model = cpu_info()
+    det = {
+        "t_ops_per_step_s": t_ops, "ops_s": rs.ops, "t_iteration_s": t_it,
+        "t_iteration_single_thread_s": t_it1, "cg_iterations_per_step": iters_per_step,
+        "cg_iterations_source": iters_source, "setup_s": rs.setup_s, "cores": cores, "cpu_model": model,
+        "value_single_thread": 1.0 / (t_ops + iters_per_step * t_it1), "extrapolated": True,
+        "sample": (f"oracle on the full layout ({rs.nc} cells, {rs.ne} edges): one calc_vel, conv_diff and "
+                   f"rot(integr_c2f) weighted 6/5/4 per step = {t_ops:.2f} s, {n_iter} PCG iteration(s) of the "
+                   f"reference recurrence at {t_it:.2f} s each ({t_it1:.2f} s with one BLAS thread), times "
+                   f"{iters_per_step:.0f} CG iterations per step ({iters_source})"),
+    }
+    return 1.0 / (t_ops + iters_per_step * t_it), det
 
 
 def full_edge_count(case):
@@ -254,29 +321,47 @@ def full_cell_count(case):
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference's CPU algorithm (the oracle port) on this host.
+
+    Rank 0 alone works.  Setup builds the oracle on the full workload layout; each
+    warm-up and timed step is one bounded sample (``reference_sample``): the step's
+    operators and one real PCG iteration at full size, scaled to the step's CG
+    iteration count, which is labelled ``extrapolated`` in the line.
+    """
     import _pyib_b200_import
     _pyib_b200_import.load()
     from pyib_b200.cases import CASES
     case = CASES[args.workload]
     if rank != 0:
         return 0
-    vals = []
-    sample = ""
+    t_run = time.perf_counter()
+    iters, source = committed_iterations_per_step(case)
+    rs = ReferenceSample(case)
+    vals, vals1, det = [], [], {}
     for k in range(args.warmup + args.steps):
-        v, sample = reference_sample(case, D32_ITERS_PER_STEP, cg_iters=2)
+        v, det = reference_sample(case, iters, source, sample=rs)
         if k >= args.warmup:
             vals.append(v)
+            vals1.append(det["value_single_thread"])
     value = float(np.mean(vals))
+    cores, model = cpu_info()
+    markers = int(case.markers()[0].shape[0])
+    det["value_single_thread"] = float(np.mean(vals1))
+    det["timed_seconds"] = time.perf_counter() - t_run
     line = {
         "impl": "reference", "metric": "D32 sphere steps/s", "value": value, "unit": "steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": case.name, "cells": full_cell_count(case), "edges": full_edge_count(case),
-                   "levels": len(case.half_widths_d), "precision": "float64",
-                   "cg_iterations_per_step": D32_ITERS_PER_STEP, "l2": "inputs larger than L2"},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample},
+                   "levels": len(case.half_widths_d), "markers": markers, "precision": "float64",
+                   "parallelism": "replicas1", "l2": "inputs larger than L2 (working set > 2 GB)",
+                   "cg_iterations_per_step": iters},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": det["sample"], "cpu_model": model,
+                         "value_one_blas_thread": det["value_single_thread"]},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "extrapolated": True, "reference_detail": det,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -306,6 +391,9 @@ def run_b200(args, world, rank, local):
     setup_s = time.perf_counter() - t_setup
     for _ in range(args.warmup):
         run.advance()
+    # the state entering the timed steps, so that the end-to-end leg repeats the same steps
+    snap = dict(s=np.asarray(run.s).copy(), s_old=np.asarray(run.s_old).copy(), state=drv.ib_state_dict(),
+                step=run.step_index, time=drv.time, loads=np.asarray(run.loads.current).copy())
     barrier(dist)
     sampler = ClockSampler(local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
     sampler.start()
@@ -327,14 +415,26 @@ def run_b200(args, world, rank, local):
     tiles = {"cell_tile": [32, 8, int(timing[3])], "node_tile": [32, 8, int(timing[4])]}
     t_dev = ev_ms.value / 1000.0
     barrier(dist)
-    # e2e: public API, host inputs and a host read of the step's load every step
-    run.loads.initialize(run.centre(drv.time))
+    # e2e: the same steps again from the same state, through the public API, with the
+    # marker positions uploaded and the step's body load read back every step
+    dev_state = dict(s=np.asarray(run.s).copy(), fE=np.asarray(drv.ib_force_E).copy())
+    run.s, run.s_old = snap["s"].copy(), snap["s_old"].copy()
+    drv.load_ib_state_dict(snap["state"])
+    drv.ib_force_update_count = snap["state"]["force_update_count"]
+    run.step_index, drv.time = snap["step"], snap["time"]
+    run.loads.current = snap["loads"].copy()
+    if run.motion is not None:
+        mk, vel = run.motion(drv.time)
+        drv.set_ib(drv.ib, mk, drv.ib_ds, vel)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         load = run.advance()
         _ = float(load["body_force"][0])
     t_e2e = time.perf_counter() - t0
     clocks = sampler.stop()
+    # the repeated steps must reproduce the device-timed ones bit for bit
+    e2e_same = bool(np.array_equal(np.asarray(run.s), dev_state["s"]) and
+                    np.array_equal(np.asarray(drv.ib_force_E), dev_state["fE"]))
     # standalone matvec timing
     mv = (C.c_double * 7)()
     sv.set("WORK_E", np.random.default_rng(0).standard_normal(sv.lay.NE) * sv.lay.edge_exists)
@@ -342,6 +442,11 @@ def run_b200(args, world, rank, local):
     mv_ms = C.c_double(mv[0])
     mv_kernels = dict(zip(["curl_interp", "curl_interp_patch", "viscous", "viscous_patch", "integr_rot_dot",
                            "integr_rot_patch_reduce"], [float(x) for x in mv[1:7]]))
+    mvf = (C.c_double * 6)()
+    sv.h.call("pyib_bench_matvec_fused", 50, C.c_double(run.dt), mvf)
+    mvf_kernels = dict(zip(["exact_vc_rows_and_list", "exact_vq_rows", "k_mvF", "exact_w_rows_dot"],
+                           [float(x) for x in mvf[1:5]]))
+    fused = os.environ.get("PYIB_FUSED_MATVEC", "0") == "1"
     ne = int(sv.lay.edge_exists.sum())
     t_dev_max = reduce_max(dist, t_dev)
     t_e2e_max = reduce_max(dist, t_e2e)
@@ -357,6 +462,7 @@ def run_b200(args, world, rank, local):
         d = json.loads(tf.read_text())
         traffic = d.get("bytes_per_edge_iteration", 0.0) * ne
     mv_achieved = ALGO_BYTES_PER_EDGE_MATVEC * ne / (mv_ms.value / 1e3) / 1e9
+    mvf_achieved = ALGO_BYTES_PER_EDGE_MATVEC * ne / (float(mvf[0]) / 1e3) / 1e9
     M = drv.ib_markers.shape[0]
     mixed = None
     if world == 1 and args.precision == "float64" and not args.no_mixed:
@@ -368,8 +474,11 @@ def run_b200(args, world, rank, local):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            v, sample = reference_sample(case, float(np.mean(iters)), cg_iters=3)
-            cpu = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample}
+            v, det = reference_sample(case, float(np.mean(iters)),
+                                      "this run's CG iterations per step on the GPU")
+            cpu = {"value": v, "unit": "steps/s", "cores": det["cores"], "kind": "port",
+                   "sample": det["sample"], "cpu_model": det["cpu_model"],
+                   "value_one_blas_thread": det["value_single_thread"], "extrapolated": True}
         line = {
             "metric": "D32 sphere steps/s", "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev_max / args.steps,
@@ -380,14 +489,19 @@ def run_b200(args, world, rank, local):
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (working set > 2 GB)",
                        "cg_iterations_per_step": float(np.mean(iters)), "setup_seconds": setup_s},
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 2 * 3 * M * 8,
-                    "d2h_bytes_per_step": 13 * 8},
+                    "d2h_bytes_per_step": 13 * 8, "same_steps_as_value": e2e_same},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "PCG iteration (matvec A/V/RI + update + direction)",
+                         "kernel": ("PCG iteration (fused matvec k_mvF with its exact rows + update + direction)"
+                                    if fused else "PCG iteration (matvec A/V/RI + update + direction)"),
                          "algorithmic_bytes_per_launch": ALGO_BYTES_PER_EDGE_ITER * ne,
                          "peak_kind": peak_kind},
-            "matvec": {"ms": mv_ms.value, "achieved_gbs": mv_achieved, "frac": mv_achieved / peak,
-                       "algorithmic_bytes": ALGO_BYTES_PER_EDGE_MATVEC * ne, "kernel_ms": mv_kernels},
+            "matvec": {"fused": {"ms": float(mvf[0]), "achieved_gbs": mvf_achieved, "frac": mvf_achieved / peak,
+                                 "kernel_ms": mvf_kernels, "node_planes_per_block": int(mvf[5])},
+                       "three_kernel": {"ms": mv_ms.value, "achieved_gbs": mv_achieved,
+                                        "frac": mv_achieved / peak, "kernel_ms": mv_kernels},
+                       "algorithmic_bytes": ALGO_BYTES_PER_EDGE_MATVEC * ne,
+                       "used_by_cg": "fused" if fused else "three_kernel"},
             "cg": {"seconds": cg_s, "iterations": cg_it, "ms_per_iteration": 1e3 * t_iter,
                    "gbs": achieved},
             "gpu_launches": launches,
@@ -402,6 +516,42 @@ def run_b200(args, world, rank, local):
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def run_matvec(args):
+    """Standalone float64 matvec timings on a workload's layout (no time stepping).
+
+    Prints one JSON line with the three-kernel matvec (``pyib_bench_matvec``) and
+    the single-pass fused matvec (``pyib_bench_matvec_fused``), each averaged over
+    50 calls with CUDA events, and their algorithmic HBM rates (16 B per edge).
+    """
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    from pyib_b200 import build
+    from pyib_b200.cases import CASES
+    from pyib_b200.device import DeviceSolver
+    build.build_library()
+    case = CASES[args.workload]
+    lay = case.layout().build()
+    sv = DeviceSolver(lay, rou=case.density, visc=case.viscosity, cavity=case.cavity)
+    sv.set("WORK_E", np.random.default_rng(0).standard_normal(lay.NE) * lay.edge_exists)
+    three = (C.c_double * 7)()
+    sv.h.call("pyib_bench_matvec", 50, C.c_double(case.time_step), three)
+    fused = (C.c_double * 6)()
+    sv.h.call("pyib_bench_matvec_fused", 50, C.c_double(case.time_step), fused)
+    ne = int(lay.edge_exists.sum())
+    peak, peak_kind = peaks()
+    gbs = lambda ms: ALGO_BYTES_PER_EDGE_MATVEC * ne / (ms / 1e3) / 1e9
+    line = {"workload": case.name, "edges": ne, "cells": int(lay.cell_active.sum()),
+            "three_kernel": {"ms": three[0], "gbs": gbs(three[0]), "kernel_ms": dict(zip(
+                ["curl_interp", "curl_interp_patch", "viscous", "viscous_patch", "integr_rot_dot",
+                 "integr_rot_patch_reduce"], list(three)[1:]))},
+            "fused": {"ms": fused[0], "gbs": gbs(fused[0]), "kz": int(fused[5]), "kernel_ms": dict(zip(
+                ["exact_vc_rows_and_list", "exact_vq_rows", "k_mvF", "exact_w_rows_dot"], list(fused)[1:5]))},
+            "peak_gbs": peak, "peak_kind": peak_kind}
+    print(json.dumps(line), flush=True)
+    sv.h.close()
     return 0
 
 
@@ -791,6 +941,8 @@ def main():
     ap.add_argument("--harmonic", action="store_true",
                     help="run --periods oscillation periods in float64 and mixed and fit the force")
     ap.add_argument("--periods", type=int, default=6)
+    ap.add_argument("--matvec-only", action="store_true",
+                    help="time the standalone float64 matvecs (three-kernel and fused) on the workload's layout")
     ap.add_argument("--compare-precision", action="store_true",
                     help="run the workload in float64 and mixed precision and report the errors")
     args = ap.parse_args()
@@ -805,6 +957,8 @@ def main():
         return run_batch(args, world, rank, local)
     if args.workload == "pressure_recovery_128":
         return run_pressure(args, world, rank, local)
+    if args.matvec_only:
+        return run_matvec(args)
     if args.compare_precision:
         return run_precision_compare(args, world, rank, local)
     if args.harmonic:

@@ -466,7 +466,7 @@ def mesh_summary(rt: CaseRuntime) -> dict:
         out.update(D_over_dx=int(mesh["cells_per_diameter"]), diameter=D, dx_fine=float(rt.dx),
                    layer_cells=per, total_cells=int(sum(per)),
                    layer_spacing_D=[float(lv.h / D) for lv in lay.levels],
-                   layer_bounds_D=[[float(lv.lo[a] / D) if s == 0 else float(lv.hi[a] / D)
+                   layer_bounds_D=[[float((lv.lo[a] + s * lv.n[a] * lv.h) / D)
                                     for a in range(3) for s in (0, 1)] for lv in lay.levels])
     return out
 
@@ -548,6 +548,35 @@ def save_field_snapshot(path: Path, rt: CaseRuntime, run_id, step, s, s_old, vc)
         kinematic_viscosity=np.float64(drv.visc / drv.rou),
     )
     _atomic_npz(path, **payload)
+
+
+def _sync_directory(directory: Path) -> None:
+    """Flush a directory entry (a rename) to disk; best effort, as on filesystems without dir fsync."""
+    try:
+        fd = os.open(directory, os.O_RDONLY)
+    except OSError:
+        return
+    try:
+        os.fsync(fd)
+    except OSError:
+        pass
+    finally:
+        os.close(fd)
+
+
+def _atomic_npz(path: Path, **arrays):
+    """Write, fsync, rename over ``path``, then fsync the directory so the rename survives a crash."""
+    tmp = path.with_name(f".{path.stem}.{uuid.uuid4().hex}.tmp.npz")
+    try:
+        np.savez(tmp, **arrays)
+        with tmp.open("r+b") as fh:
+            fh.flush()
+            os.fsync(fh.fileno())
+        os.replace(tmp, path)
+        _sync_directory(path.parent)
+    finally:
+        if tmp.exists():
+            tmp.unlink()
 
 
 def _str(d, k):

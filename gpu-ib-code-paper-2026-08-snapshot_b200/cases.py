@@ -23,6 +23,8 @@ R = 0.25
 
 def fibonacci_sphere(count, radius, centre):
     """Fibonacci-lattice surface points (the layout of ``ib_case.py:554-563``)."""
+    if count < 4:
+        raise ValueError("a sphere surface requires at least four markers")
     k = np.arange(count, dtype=np.float64)
     polar = np.arccos(1.0 - 2.0 * (k + 0.5) / count)
     azim = np.pi * (1.0 + np.sqrt(5.0)) * k

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -34,6 +35,10 @@ constexpr int kSlots = 16;               // reduction values per block
 // structured stencil tiles: 32 x 8 threads in (x, y), each marching KZ planes in z
 constexpr int TX = 32, TY = 8;
 constexpr int kTargetBlocks = 148 * 16;   // z-chunk depth is chosen to give at least this many tiles
+// fused matvec blocks: 32 x 16 threads over a column tile with a 2-column halo below and
+// 1 above, owning 29 x 13 node columns; at most kMaxKzF node planes per block
+constexpr int FX = 32, FY = 16, FOX = FX - 3, FOY = FY - 3;
+constexpr int kMaxKzF = 32;
 
 struct LevelMeta {
   int n[3];
@@ -49,6 +54,8 @@ struct LevelMeta {
   int plane_base;      // first per-plane partial-sum slot of this level (kernel RI)
   int zbA;             // first z-block of this level in the cell-tile grids
   int zbR;             // first z-block of this level in the node-tile grid
+  int zbF;             // first z-block of this level in the fused-matvec grid
+  int fplane_base;     // first per-plane partial-sum slot of this level (fused matvec)
 };
 
 struct Meta {
@@ -63,6 +70,9 @@ struct Meta {
   int nplanes;         // per-plane partial sums of kernel RI (independent of the z-chunk depth)
   int ri_up;           // 1: kernel RI also marches the upper-face nodes (i = nx, j = ny, k = nz);
                        // 0: every upper-face edge is an exact (patch) row or masked
+  int kzF;             // node planes marched by one block of the fused matvec
+  int gxF, gyF, gzF;   // fused-matvec grid
+  int nplanesF;        // per-plane partial sums of the fused matvec
 };
 
 struct CGState {
@@ -139,6 +149,14 @@ struct pyib_ctx {
   int cg_graph_check = 0;
   long long cg_graph_kernels = 0;    // kernel nodes in cg_graph
   int cg_graph_alpd = -1;
+  // fused single-pass matvec of the float64 CG (k_mvF)
+  bool use_fused = false;        // PYIB_FUSED_MATVEC=1 selects the single-pass matvec in the CG
+  bool fused_ready = false;
+  bool tunedF = false;
+  unsigned int *f_irrA = nullptr, *f_irrV = nullptr, *f_needR = nullptr;
+  unsigned char* f_flags = nullptr;   // per cell: exact vc / exact vq / store vq
+  int* f_list = nullptr;         // regular cells whose template vc an exact V row reads
+  long long n_list = 0;
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
   double cg_seconds = 0.0;
@@ -316,6 +334,26 @@ void set_grids(Meta& m, int kzA, int kzR) {
     pb += gxR * gyR * (m.lv[L].n[2] + m.ri_up);
   }
   m.nplanes = pb;
+}
+
+// Grid of the fused matvec for z-chunk depth kzF (node planes per block).
+void set_grids_fused(Meta& m, int kzF) {
+  m.kzF = kzF;
+  int z = 0, gx = 1, gy = 1;
+  for (int L = 0; L < m.nl; ++L) {
+    LevelMeta& l = m.lv[L];
+    l.zbF = z;
+    z += (l.n[2] + m.ri_up + kzF - 1) / kzF;
+    gx = std::max(gx, (l.n[0] + m.ri_up + FOX - 1) / FOX);
+    gy = std::max(gy, (l.n[1] + m.ri_up + FOY - 1) / FOY);
+  }
+  m.gxF = gx; m.gyF = gy; m.gzF = z;
+  int pb = 0;
+  for (int L = 0; L < m.nl; ++L) {
+    m.lv[L].fplane_base = pb;
+    pb += gx * gy * (m.lv[L].n[2] + m.ri_up);
+  }
+  m.nplanesF = pb;
 }
 
 // ---------------------------------------------------------------------------
@@ -726,6 +764,444 @@ __global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* _
     st->pw = acc[0];
     st->alpha = st->eta / (acc[0] != 0.0 ? acc[0] : INFINITY);
     st->counter = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused single-pass float64 matvec: w = R I V P C p and the dot p.w in one kernel.
+//
+// Block of FX x FY = 32 x 16 threads; thread (tx, ty) owns the cell/node column
+// (I, J) = (FOX*bx - 2 + tx, FOY*by - 2 + ty) of one level and marches z.  At node
+// plane k the block computes, in registers and shared memory only:
+//   vc(k+1) = P C p on every column            (12 edge loads per cell, L1)
+//   vq(k)   = V vc on columns 1 <= tx, ty < 31/15   (x neighbours by shuffle,
+//             y neighbours from shared memory, z neighbours in registers)
+//   w(k)    = R I vq on the owned nodes 2 <= tx < 31, 2 <= ty < 15  (29 x 13)
+// so the cell intermediates vc and vq never reach DRAM: the kernel reads p once
+// (each tile stages its planes of p, halo included, into shared memory with
+// cp.async two planes ahead of use) and writes w once.  The arithmetic of every template row
+// is the expression of k_mvA / k_mvV / ri_plane, term for term, so w is bit-identical
+// to the three-kernel path.  Rows the templates cannot reproduce keep their exact
+// CSR rows: k_patchA (vc of irregular cells) and k_vc_list (template vc of the
+// cells those rows read) and k_patchV (vq of irregular cells) run before, into the
+// same vcm / vq buffers, and this kernel takes vc / vq of a flagged cell from there;
+// it also stores the template vq of the cells that the exact w rows of k_patchRI
+// read, and k_patchRI runs after it as in the three-kernel path.
+// ---------------------------------------------------------------------------
+
+struct FusedTabs {
+  const unsigned int* irrA;    // cell bits: exact vc in vcm (k_patchA)
+  const unsigned int* irrV;    // cell bits: exact vq in vq (k_patchV)
+  const unsigned int* needR;   // cell bits: k_patchRI reads this cell's vq
+  const unsigned int* pbits;   // edge bits: exact (patch) w rows, outside the template dot
+  const unsigned char* flags;  // the three cell bits as one byte per cell (k_cell_flags)
+};
+
+__device__ __forceinline__ int level_of_zblock_fused(const Meta& m, int bz) {
+  int L = 0;
+  while (L + 1 < m.nl && bz >= m.lv[L + 1].zbF) ++L;
+  return L;
+}
+
+// template vc of cell (i, j, k) of level l (the arithmetic of k_mvA)
+__device__ __forceinline__ void vc_template(const LevelMeta& l, const double* __restrict__ p, int i, int j, int k,
+                                            double& vx, double& vy, double& vz) {
+  const int nx = l.n[0], ny = l.n[1];
+  const double* ex = p + l.ebase[0];
+  const double* ey = p + l.ebase[1];
+  const double* ez = p + l.ebase[2];
+  const int sxk = (ny + 1) * nx, syk = ny * (nx + 1);
+  const int ox = (k * (ny + 1) + j) * nx + i;
+  const int oy = (k * ny + j) * (nx + 1) + i;
+  const int oz = (k * (ny + 1) + j) * (nx + 1) + i;
+  const double ex00 = ex[ox], ex10 = ex[ox + nx], ex01 = ex[ox + sxk], ex11 = ex[ox + sxk + nx];
+  const double ey00 = ey[oy], ey10 = ey[oy + 1], ey01 = ey[oy + syk], ey11 = ey[oy + syk + 1];
+  const double ez00 = ez[oz], ez10 = ez[oz + 1], ez01 = ez[oz + nx + 1], ez11 = ez[oz + nx + 2];
+  const double s = 1.0 / (2.0 * l.h * l.h);
+  const double ux0 = ey00 + ez01 - ey01 - ez00;
+  const double ux1 = ey10 + ez11 - ey11 - ez10;
+  const double uy0 = ez00 + ex01 - ez10 - ex00;
+  const double uy1 = ez01 + ex11 - ez11 - ex10;
+  const double uz0 = ex00 + ey10 - ex10 - ey00;
+  const double uz1 = ex01 + ey11 - ex11 - ey01;
+  vx = (ux0 + ux1) * s;
+  vy = (uy0 + uy1) * s;
+  vz = (uz0 + uz1) * s;
+}
+
+// Shared-memory staging of p: one node plane of the tile holds the x-edges of
+// 32 x 17 node columns, the y-edges of 33 x 16 and the z-edges of 33 x 17 (the
+// 12 edges of every cell of the 32 x 16 column block).  Planes are copied with
+// cp.async two planes ahead of their use into a ring of kPRing planes, so the
+// loads of a plane are in flight while the block computes the previous ones.
+// Each block tabulates once, in shared memory, the in-plane source offset of
+// every staged element (or -1 outside the level box), so a plane's copies cost a
+// table read, one multiply-add and the copy instruction each.
+constexpr int FPX = FX + 1, FPY = FY + 1;
+constexpr int kPEx = FX * FPY;                  // 544 x-edges a plane
+constexpr int kPEy = FPX * FY;                  // 528 y-edges
+constexpr int kPEz = FPX * FPY;                 // 561 z-edges
+constexpr int kPPlane = kPEx + kPEy + kPEz;     // 1633 doubles
+constexpr int kPRing = 5;
+constexpr int kPIter = (kPPlane + FX * FY - 1) / (FX * FY);   // staged elements per thread and plane
+constexpr size_t kFusedSmemBytes =
+    (size_t)(kPRing * kPPlane + 2 * 3 * FY * FX + 3 * FY * FX + kMaxKzF * FY) * sizeof(double) +
+    (size_t)kPPlane * sizeof(int);
+
+// cell flags of the fused matvec (one byte per cell)
+constexpr unsigned char kFlagExactVc = 1, kFlagExactVq = 2, kFlagStoreVq = 4;
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = ok ? 8 : 0;   // 0 source bytes: the 8 destination bytes are zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ int ring_slot(int kp) { return ((kp % kPRing) + kPRing) % kPRing; }
+
+// In-plane source offsets of the staged elements of the tile whose column (0, 0)
+// is (x0, y0): offset of the edge within its array's plane, -1 outside the box.
+__device__ __forceinline__ void tabulate_p_offsets(const LevelMeta& l, int* s_poff, int x0, int y0, int tid) {
+  const int nx = l.n[0], ny = l.n[1];
+  for (int q = tid; q < kPPlane; q += FX * FY) {
+    int off = -1;
+    if (q < kPEx) {
+      const int yy = q / FX, xx = q - yy * FX, I = x0 + xx, J = y0 + yy;
+      if (I >= 0 && I < nx && J >= 0 && J <= ny) off = J * nx + I;
+    } else if (q < kPEx + kPEy) {
+      const int r = q - kPEx, yy = r / FPX, xx = r - yy * FPX, I = x0 + xx, J = y0 + yy;
+      if (I >= 0 && I <= nx && J >= 0 && J < ny) off = J * (nx + 1) + I;
+    } else {
+      const int r = q - kPEx - kPEy, yy = r / FPX, xx = r - yy * FPX, I = x0 + xx, J = y0 + yy;
+      if (I >= 0 && I <= nx && J >= 0 && J <= ny) off = J * (nx + 1) + I;
+    }
+    s_poff[q] = off;
+  }
+}
+
+// Issue the copies of node plane kp into ring slot `slot`; elements outside the
+// level box (offset -1) or its planes are zero-filled.
+__device__ __forceinline__ void load_p_plane(const LevelMeta& l, const double* __restrict__ p, double* slot,
+                                             const int* s_poff, int kp, int tid) {
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const bool pxy = kp >= 0 && kp <= nz, pz = kp >= 0 && kp < nz;
+  const double* bx = p + l.ebase[0] + (pxy ? kp * ((ny + 1) * nx) : 0);
+  const double* by = p + l.ebase[1] + (pxy ? kp * (ny * (nx + 1)) : 0);
+  const double* bz = p + l.ebase[2] + (pz ? kp * ((ny + 1) * (nx + 1)) : 0);
+#pragma unroll
+  for (int u = 0; u < kPIter; ++u) {
+    const int q = tid + u * FX * FY;
+    if (q < kPPlane) {
+      const int off = s_poff[q];
+      const double* base = q < kPEx ? bx : (q < kPEx + kPEy ? by : bz);
+      const bool ok = off >= 0 && (q < kPEx + kPEy ? pxy : pz);
+      cp_async8(slot + q, ok ? base + off : p, ok);
+    }
+  }
+}
+
+// template vc of the cell of column (tx, ty) on plane kc from the staged planes kc and
+// kc + 1 (the arithmetic of k_mvA); s = 1 / (2 h^2)
+__device__ __forceinline__ void vc_staged(const double* pa, const double* pb, int tx, int ty, double s,
+                                          double& vx, double& vy, double& vz) {
+  const double ex00 = pa[ty * FX + tx], ex10 = pa[(ty + 1) * FX + tx];
+  const double ex01 = pb[ty * FX + tx], ex11 = pb[(ty + 1) * FX + tx];
+  const double* ya = pa + kPEx;
+  const double* yb = pb + kPEx;
+  const double ey00 = ya[ty * FPX + tx], ey10 = ya[ty * FPX + tx + 1];
+  const double ey01 = yb[ty * FPX + tx], ey11 = yb[ty * FPX + tx + 1];
+  const double* za = pa + kPEx + kPEy;
+  const double ez00 = za[ty * FPX + tx], ez10 = za[ty * FPX + tx + 1];
+  const double ez01 = za[(ty + 1) * FPX + tx], ez11 = za[(ty + 1) * FPX + tx + 1];
+  const double ux0 = ey00 + ez01 - ey01 - ez00;
+  const double ux1 = ey10 + ez11 - ey11 - ez10;
+  const double uy0 = ez00 + ex01 - ez10 - ex00;
+  const double uy1 = ez01 + ex11 - ez11 - ex10;
+  const double uz0 = ex00 + ey10 - ex10 - ey00;
+  const double uz1 = ex01 + ey11 - ex11 - ey01;
+  vx = (ux0 + ux1) * s;
+  vy = (uy0 + uy1) * s;
+  vz = (uz0 + uz1) * s;
+}
+
+__global__ void __launch_bounds__(FX * FY, 2) k_mvF(Meta m, const double* __restrict__ p, double* __restrict__ w,
+                                                   const double* __restrict__ vcm, double* vq, FusedTabs tb,
+                                                   double* partials, const CGState* __restrict__ st, int do_dot) {
+  if (st->done) return;
+  extern __shared__ double fsm[];
+  double* ring = fsm;                                                   // [kPRing][kPPlane]
+  double (*s_vc)[3][FY][FX] = reinterpret_cast<double (*)[3][FY][FX]>(fsm + kPRing * kPPlane);
+  double (*s_vq)[FY][FX] = reinterpret_cast<double (*)[FY][FX]>(fsm + kPRing * kPPlane + 2 * 3 * FY * FX);
+  double (*s_dot)[FY] = reinterpret_cast<double (*)[FY]>(fsm + kPRing * kPPlane + 2 * 3 * FY * FX + 3 * FY * FX);
+  int* s_poff = reinterpret_cast<int*>(fsm + kPRing * kPPlane + 2 * 3 * FY * FX + 3 * FY * FX + kMaxKzF * FY);
+  const int L = level_of_zblock_fused(m, blockIdx.z);
+  const LevelMeta& l = m.lv[L];
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + FX * ty;
+  const int x0 = blockIdx.x * FOX - 2, y0 = blockIdx.y * FOY - 2;
+  const int I = x0 + tx, J = y0 + ty;
+  const int k0 = (blockIdx.z - l.zbF) * m.kzF;
+  const int k1 = min(k0 + m.kzF, nz + m.ri_up);
+  const int nc = (int)m.nc;
+  const bool col = I >= 0 && I < nx && J >= 0 && J < ny;
+  const bool col_hole = l.has_hole && I >= l.hole_lo[0] && I < l.hole_hi[0] && J >= l.hole_lo[1] &&
+                        J < l.hole_hi[1];
+  const int hz0 = col_hole ? l.hole_lo[2] : 0, hz1 = col_hole ? l.hole_hi[2] : 0;
+  const bool do_vq = tx >= 1 && tx < FX - 1 && ty >= 1 && ty < FY - 1;
+  const bool own = tx >= 2 && tx < FX - 1 && ty >= 2 && ty < FY - 1;      // owned node (I >= 0, J >= 0)
+  const bool do_w = own && I < nx + m.ri_up && J < ny + m.ri_up;
+  const double rou = st->rou, kf = st->kfac;
+  const double inv_h2 = 1.0 / (l.h * l.h);
+  const double s_a = 1.0 / (2.0 * l.h * l.h);
+  const double hh = 0.5 * l.h;
+  const int cplane = nx * ny;
+  const int ccol = (int)l.cbase + J * nx + I;     // cell id of (I, J, 0)
+  const int exs = (ny + 1) * nx, eys = ny * (nx + 1), ezs = (ny + 1) * (nx + 1);
+  const int ex0 = (int)l.ebase[0] + J * nx + I, ey0 = (int)l.ebase[1] + J * (nx + 1) + I,
+            ez0 = (int)l.ebase[2] + J * (nx + 1) + I;   // edges of node (I, J, 0)
+
+  auto cell_in = [&](int kc) { return col && kc >= 0 && kc < nz && !(kc >= hz0 && kc < hz1); };
+  auto flag_of = [&](int kc) -> unsigned int { return cell_in(kc) ? tb.flags[ccol + kc * cplane] : 0u; };
+  auto inc = [](int s) { return s + 1 == kPRing ? 0 : s + 1; };
+
+  tabulate_p_offsets(l, s_poff, x0, y0, tid);
+  __syncthreads();
+  // node planes k0-2 .. k0+1 (one group) and k0+2 (a second group)
+  for (int kp = k0 - 2; kp <= k0 + 1; ++kp) load_p_plane(l, p, ring + ring_slot(kp) * kPPlane, s_poff, kp, tid);
+  cp_async_commit();
+  load_p_plane(l, p, ring + ring_slot(k0 + 2) * kPPlane, s_poff, k0 + 2, tid);
+  cp_async_commit();
+  unsigned int fm = flag_of(k0 - 2), f0 = flag_of(k0 - 1), f1 = flag_of(k0);
+  cp_async_wait<1>();
+  __syncthreads();
+  double am[3] = {0.0, 0.0, 0.0}, a0[3] = {0.0, 0.0, 0.0}, ap[3];
+  {
+    // vc on planes k0-2 and k0-1
+    const int sa = ring_slot(k0 - 2), sb = inc(sa), sc = inc(sb);
+    if (cell_in(k0 - 2)) {
+      const int c = ccol + (k0 - 2) * cplane;
+      if (fm & kFlagExactVc) {
+        am[0] = vcm[c]; am[1] = vcm[nc + c]; am[2] = vcm[2 * nc + c];
+      } else {
+        vc_staged(ring + sa * kPPlane, ring + sb * kPPlane, tx, ty, s_a, am[0], am[1], am[2]);
+      }
+    }
+    if (cell_in(k0 - 1)) {
+      const int c = ccol + (k0 - 1) * cplane;
+      if (f0 & kFlagExactVc) {
+        a0[0] = vcm[c]; a0[1] = vcm[nc + c]; a0[2] = vcm[2 * nc + c];
+      } else {
+        vc_staged(ring + sb * kPPlane, ring + sc * kPPlane, tx, ty, s_a, a0[0], a0[1], a0[2]);
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) s_vc[(k0 - 1) & 1][d][ty][tx] = a0[d];
+  __syncthreads();
+  // carried values of node (I, J) from plane k-1 (ri_plane's RICarry)
+  double c_vz00 = 0.0, c_vzm0 = 0.0, c_vz0m = 0.0, c_fx = 0.0, c_fy = 0.0;
+  int sk = ring_slot(k0 - 1);          // ring slot of node plane k
+  for (int k = k0 - 1; k < k1; ++k) {
+    const int sk1 = inc(sk), sk2 = inc(sk1), skm = sk == 0 ? kPRing - 1 : sk - 1;   // planes k+1, k+2, k-1
+    // global words this step needs, issued first: the next cell's flags and the
+    // patch-row bits of this node's w rows
+    const unsigned int f2 = flag_of(k + 2);
+    const bool wk = do_w && k >= k0 && do_dot;
+    const int ex_e = ex0 + k * exs, ey_e = ey0 + k * eys, ez_e = ez0 + k * ezs;
+    const unsigned int bwx = (wk && I < nx) ? tb.pbits[ex_e >> 5] : 0u;
+    const unsigned int bwy = (wk && J < ny) ? tb.pbits[ey_e >> 5] : 0u;
+    const unsigned int bwz = (wk && k < nz) ? tb.pbits[ez_e >> 5] : 0u;
+    // ---- vc(I, J, k+1) from the staged planes k+1, k+2 ---------------------------
+    ap[0] = ap[1] = ap[2] = 0.0;
+    if (cell_in(k + 1)) {
+      const int c = ccol + (k + 1) * cplane;
+      if (f1 & kFlagExactVc) {
+        ap[0] = vcm[c]; ap[1] = vcm[nc + c]; ap[2] = vcm[2 * nc + c];
+      } else {
+        vc_staged(ring + sk1 * kPPlane, ring + sk2 * kPPlane, tx, ty, s_a, ap[0], ap[1], ap[2]);
+      }
+    }
+    const int sl = (k + 1) & 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s_vc[sl][d][ty][tx] = ap[d];
+    __syncthreads();
+    // plane k+4 into the ring slot of plane k-1 (last read before this barrier)
+    load_p_plane(l, p, ring + skm * kPPlane, s_poff, k + 4, tid);
+    cp_async_commit();
+    // ---- vq(I, J, k) ---------------------------------------------------------------
+    double xp[3], xm[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      xp[d] = __shfl_down_sync(0xffffffffu, a0[d], 1);
+      xm[d] = __shfl_up_sync(0xffffffffu, a0[d], 1);
+    }
+    if (do_vq) {
+      double q[3] = {0.0, 0.0, 0.0};
+      if (cell_in(k)) {
+        const int c = ccol + k * cplane;
+        if (f0 & kFlagExactVq) {
+          q[0] = vq[c];
+          q[1] = vq[nc + c];
+          q[2] = vq[2 * nc + c];
+        } else {
+          const int s0 = k & 1;
+          const bool xpn = I + 1 < nx, xmn = I > 0, ypn = J + 1 < ny, ymn = J > 0, zpn = k + 1 < nz, zmn = k > 0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double x0v = a0[d];
+            double acc = 0;
+            acc += xpn ? xp[d] - x0v : -2 * x0v;
+            acc += xmn ? xm[d] - x0v : -2 * x0v;
+            acc += ypn ? s_vc[s0][d][ty + 1][tx] - x0v : -2 * x0v;
+            acc += ymn ? s_vc[s0][d][ty - 1][tx] - x0v : -2 * x0v;
+            acc += zpn ? ap[d] - x0v : -2 * x0v;
+            acc += zmn ? am[d] - x0v : -2 * x0v;
+            q[d] = rou * x0v - kf * (acc * inv_h2);
+          }
+          // the exact w rows of k_patchRI read this cell's vq: the owner stores it
+          if (own && k >= k0 && (f0 & kFlagStoreVq)) {
+            vq[c] = q[0];
+            vq[nc + c] = q[1];
+            vq[2 * nc + c] = q[2];
+          }
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) s_vq[d][ty][tx] = q[d];
+    }
+    cp_async_wait<1>();   // this thread's copies of plane k+3 have landed
+    __syncthreads();
+    // ---- w on node plane k (ri_plane with vq from shared memory) ---------------------
+    if (k >= k0) {
+      double dot = 0.0;
+      if (do_w) {
+        const int i = I, j = J;
+        const bool c00 = i < nx && j < ny, cm0 = i > 0 && i <= nx && j < ny, c0m = i < nx && j > 0 && j <= ny,
+                   cmm = i > 0 && j > 0 && i <= nx && j <= ny;
+        const bool zin = k < nz;
+        // p of the node's three edges from the staged plane k (the dot's left factor)
+        const double* pk = ring + sk * kPPlane;
+        const double px = (do_dot && i < nx) ? pk[ty * FX + tx] : 0.0;
+        const double py = (do_dot && j < ny) ? pk[kPEx + ty * FPX + tx] : 0.0;
+        const double pz = (do_dot && zin) ? pk[kPEx + kPEy + ty * FPX + tx] : 0.0;
+        const double vz00 = (zin && c00) ? s_vq[2][ty][tx] : 0.0;
+        const double vzm0 = (zin && cm0) ? s_vq[2][ty][tx - 1] : 0.0;
+        const double vz0m = (zin && c0m) ? s_vq[2][ty - 1][tx] : 0.0;
+        double fx = 0, fy = 0, fx_jm = 0, fy_im = 0;
+        if (zin) {
+          const double vx00 = c00 ? s_vq[0][ty][tx] : 0.0, vxm0 = cm0 ? s_vq[0][ty][tx - 1] : 0.0;
+          const double vy00 = c00 ? s_vq[1][ty][tx] : 0.0, vy0m = c0m ? s_vq[1][ty - 1][tx] : 0.0;
+          if (j < ny) fx = hh * (vxm0 + vx00);
+          if (i < nx) fy = hh * (vy0m + vy00);
+          if (j > 0) fx_jm = hh * ((cmm ? s_vq[0][ty - 1][tx - 1] : 0.0) + (c0m ? s_vq[0][ty - 1][tx] : 0.0));
+          if (i > 0) fy_im = hh * ((cmm ? s_vq[1][ty - 1][tx - 1] : 0.0) + (cm0 ? s_vq[1][ty][tx - 1] : 0.0));
+        }
+        const double fz = (i < nx && j < ny) ? hh * (c_vz00 + vz00) : 0.0;
+        const double fz_im = (i > 0 && j < ny) ? hh * (c_vzm0 + vzm0) : 0.0;
+        const double fz_jm = (i < nx && j > 0) ? hh * (c_vz0m + vz0m) : 0.0;
+        if (i < nx) {
+          const double val = fz - fz_jm + c_fy - fy;
+          w[ex_e] = val;
+          if (!((bwx >> (ex_e & 31)) & 1u)) dot += px * val;
+        }
+        if (j < ny) {
+          const double val = fx - c_fx + fz_im - fz;
+          w[ey_e] = val;
+          if (!((bwy >> (ey_e & 31)) & 1u)) dot += py * val;
+        }
+        if (zin) {
+          const double val = fy - fy_im + fx_jm - fx;
+          w[ez_e] = val;
+          if (!((bwz >> (ez_e & 31)) & 1u)) dot += pz * val;
+        }
+        c_vz00 = vz00; c_vzm0 = vzm0; c_vz0m = vz0m;
+        c_fx = fx; c_fy = fy;
+      }
+      if (do_dot) {
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
+        if (tx == 0) s_dot[k - k0][ty] = dot;
+      }
+    } else if (do_w) {
+      // plane k0 - 1: only the carried values of node (I, J)
+      const int i = I, j = J;
+      const bool c00 = i < nx && j < ny, cm0 = i > 0 && i <= nx && j < ny, c0m = i < nx && j > 0 && j <= ny;
+      const bool zin = k >= 0 && k < nz;
+      c_vz00 = (zin && c00) ? s_vq[2][ty][tx] : 0.0;
+      c_vzm0 = (zin && cm0) ? s_vq[2][ty][tx - 1] : 0.0;
+      c_vz0m = (zin && c0m) ? s_vq[2][ty - 1][tx] : 0.0;
+      c_fx = c_fy = 0.0;
+      if (zin) {
+        if (i < nx) c_fy = hh * ((c0m ? s_vq[1][ty - 1][tx] : 0.0) + (c00 ? s_vq[1][ty][tx] : 0.0));
+        if (j < ny) c_fx = hh * ((cm0 ? s_vq[0][ty][tx - 1] : 0.0) + (c00 ? s_vq[0][ty][tx] : 0.0));
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      am[d] = a0[d];
+      a0[d] = ap[d];
+    }
+    f0 = f1;
+    f1 = f2;
+    sk = sk1;
+  }
+  cp_async_wait<0>();   // no copy may still target this block's shared memory at exit
+  if (!do_dot) return;
+  __syncthreads();
+  // one partial per (level, tile, node plane), its 16 warp sums combined in a fixed
+  // order: the dot does not depend on the z-chunk depth the autotuner picked
+  if (tid < k1 - k0) {
+    const double* q = s_dot[tid];
+    const double v = (((q[0] + q[8]) + (q[4] + q[12])) + ((q[2] + q[10]) + (q[6] + q[14]))) +
+                     (((q[1] + q[9]) + (q[5] + q[13])) + ((q[3] + q[11]) + (q[7] + q[15])));
+    partials[l.fplane_base + ((long long)(k0 + tid) * m.gyF + blockIdx.y) * m.gxF + blockIdx.x] = v;
+  }
+}
+
+// flag byte per cell from the three bit arrays (kFlagExactVc | kFlagExactVq | kFlagStoreVq)
+__global__ void k_cell_flags(long long nc, const unsigned int* __restrict__ a, const unsigned int* __restrict__ v,
+                             const unsigned int* __restrict__ r, unsigned char* flags) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
+       c += (long long)gridDim.x * blockDim.x) {
+    unsigned int f = 0;
+    if (bit_set(a, c)) f |= kFlagExactVc;
+    if (bit_set(v, c)) f |= kFlagExactVq;
+    if (bit_set(r, c)) f |= kFlagStoreVq;
+    flags[c] = (unsigned char)f;
+  }
+}
+
+// template vc of listed regular cells whose vc an exact V row reads (k_patchV)
+__global__ void __launch_bounds__(kThreads) k_vc_list(Meta m, long long n, const int* __restrict__ cells,
+                                                      const double* __restrict__ p, double* vcm,
+                                                      const CGState* __restrict__ st) {
+  if (st->done) return;
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int c = cells[q];
+  int L = 0;
+  while (L + 1 < m.nl && c >= m.lv[L + 1].cbase) ++L;
+  const LevelMeta& l = m.lv[L];
+  const int loc = c - (int)l.cbase;
+  const int i = loc % l.n[0], j = (loc / l.n[0]) % l.n[1], k = loc / (l.n[0] * l.n[1]);
+  double vx, vy, vz;
+  vc_template(l, p, i, j, k, vx, vy, vz);
+  vcm[c] = vx;
+  vcm[m.nc + c] = vy;
+  vcm[2 * m.nc + c] = vz;
+}
+
+// setup: cell bits from a list of cell ids (or of component-major vq columns)
+__global__ void k_mark_cells(long long n, const int* __restrict__ ids, long long nc, unsigned int* bits) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    long long c = ids[q];
+    c %= nc;
+    atomicOr(&bits[c >> 5], 1u << (c & 31));
   }
 }
 
@@ -1898,6 +2374,144 @@ int launch_matvec(pyib_ctx* ctx, const double* in, double* out, int alpd, int do
                                  tp<double>(ctx, PYIB_T_PR_VAL));
 }
 
+// Flags and lists of the fused matvec, from the patch tables (once per table upload):
+// irrA / irrV = cells with exact vc / vq rows, needR = cells whose vq an exact w row
+// reads, and the list of regular cells whose template vc an exact vq row reads.
+int prepare_fused(pyib_ctx* ctx) {
+  if (ctx->fused_ready) return PYIB_OK;
+  const long long nc = ctx->lay.ncell, words = (nc + 31) / 32;
+  unsigned int** bits[] = {&ctx->f_irrA, &ctx->f_irrV, &ctx->f_needR};
+  for (unsigned int** b : bits) {
+    if (*b) { CK(cudaFree(*b)); *b = nullptr; }
+    RET(alloc(ctx, (void**)b, words * sizeof(unsigned int)));
+  }
+  if (ctx->f_list) { CK(cudaFree(ctx->f_list)); ctx->f_list = nullptr; }
+  if (ctx->nA > 0) {
+    k_mark_cells<<<grid_for(ctx->nA), kThreads, 0, ctx->stream>>>(ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), nc,
+                                                                    ctx->f_irrA);
+    CKL();
+  }
+  if (ctx->nV > 0) {
+    k_mark_cells<<<grid_for(ctx->nV), kThreads, 0, ctx->stream>>>(ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), nc,
+                                                                    ctx->f_irrV);
+    CKL();
+  }
+  if (ctx->nR > 0) {
+    const long long nnz = (long long)(ctx->tab[PYIB_T_PR_COL].bytes / sizeof(int));
+    k_mark_cells<<<grid_for(nnz), kThreads, 0, ctx->stream>>>(nnz, tp<int>(ctx, PYIB_T_PR_COL), nc, ctx->f_needR);
+    CKL();
+  }
+  if (ctx->f_flags) { CK(cudaFree(ctx->f_flags)); ctx->f_flags = nullptr; }
+  RET(alloc(ctx, (void**)&ctx->f_flags, nc));
+  k_cell_flags<<<grid_for(nc), kThreads, 0, ctx->stream>>>(nc, ctx->f_irrA, ctx->f_irrV, ctx->f_needR,
+                                                           ctx->f_flags);
+  CKL();
+  // cells read by the exact V rows (their columns and the rows' own cells), minus the
+  // cells with exact vc: a host pass over the column list
+  std::vector<int> cols;
+  if (ctx->nV > 0) {
+    const size_t nnz = ctx->tab[PYIB_T_PV_COL].bytes / sizeof(int);
+    cols.resize(nnz + ctx->nV);
+    CK(cudaMemcpyAsync(cols.data(), tp<int>(ctx, PYIB_T_PV_COL), nnz * sizeof(int), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(cols.data() + nnz, tp<int>(ctx, PYIB_T_PV_IDS), ctx->nV * sizeof(int),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  std::vector<unsigned int> irrA(words);
+  CK(cudaMemcpyAsync(irrA.data(), ctx->f_irrA, words * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<char> want(nc, 0);
+  for (int c : cols)
+    if (c >= 0 && c < nc && !((irrA[c >> 5] >> (c & 31)) & 1u)) want[c] = 1;
+  std::vector<int> list;
+  for (long long c = 0; c < nc; ++c)
+    if (want[c]) list.push_back((int)c);
+  ctx->n_list = (long long)list.size();
+  RET(alloc(ctx, (void**)&ctx->f_list, std::max<size_t>(1, list.size()) * sizeof(int)));
+  if (!list.empty())
+    CK(cudaMemcpyAsync(ctx->f_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if ((long long)ctx->meta.nplanesF + patch_grid(ctx->nR) > kPartStride)
+    return set_err(ctx, PYIB_E_ARG, "too many reduction slots for the fused matvec");
+  CK(cudaFuncSetAttribute(k_mvF, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemBytes));
+  ctx->fused_ready = true;
+  return PYIB_OK;
+}
+
+// The float64 matvec as one pass: exact vc / vq rows first, then k_mvF, then the exact
+// w rows with the final dot (alpha = eta / p.w when do_dot).
+int launch_matvec_fused(pyib_ctx* ctx, const double* in, double* out, int do_dot) {
+  RET(prepare_fused(ctx));
+  const Meta& m = ctx->meta;
+  const long long nc = ctx->lay.ncell;
+  if (ctx->nA > 0) {
+    k_patchA<double><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
+        ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR), tp<int>(ctx, PYIB_T_PA_COL),
+        tp<double>(ctx, PYIB_T_PA_VAL), in, ctx->vcm, nc, ctx->st);
+    CKL();
+  }
+  if (ctx->n_list > 0) {
+    k_vc_list<<<patch_grid(ctx->n_list), kThreads, 0, ctx->stream>>>(m, ctx->n_list, ctx->f_list, in, ctx->vcm,
+                                                                      ctx->st);
+    CKL();
+  }
+  if (ctx->nV > 0) {
+    k_patchV<double><<<patch_grid(ctx->nV), kThreads, 0, ctx->stream>>>(
+        ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL),
+        tp<double>(ctx, PYIB_T_PV_VAL), ctx->vcm, ctx->vq, nc, ctx->st);
+    CKL();
+  }
+  const FusedTabs tb{ctx->f_irrA, ctx->f_irrV, ctx->f_needR, tp<unsigned int>(ctx, PYIB_T_PR_BITS),
+                     ctx->f_flags};
+  k_mvF<<<dim3(m.gxF, m.gyF, m.gzF), dim3(FX, FY, 1), kFusedSmemBytes, ctx->stream>>>(m, in, out, ctx->vcm, ctx->vq, tb,
+                                                                       ctx->partials, ctx->st, do_dot);
+  CKL();
+  k_patchRI<double><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
+      ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL),
+      tp<double>(ctx, PYIB_T_PR_VAL), ctx->vq, out, in, ctx->partials, m.nplanesF, ctx->st, do_dot);
+  CKL();
+  return PYIB_OK;
+}
+
+// Depth of the fused matvec's z chunks, by timing 4, 8, 16 and 32 node planes.
+int tune_fused(pyib_ctx* ctx) {
+  if (ctx->tunedF) return PYIB_OK;
+  RET(prepare_fused(ctx));
+  CGState h{};
+  CK(cudaMemcpyAsync(&h, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CGState t = h;
+  t.rou = 1.0;
+  t.kfac = 1e-3;
+  t.done = 0;
+  t.counter = 0u;
+  CK(cudaMemcpyAsync(ctx->st, &t, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  const int depths[4] = {4, 8, 16, 32};
+  int bestZ = 16;
+  double best = 1e30;
+  for (int a = 0; a < 4; ++a) {
+    set_grids_fused(ctx->meta, depths[a]);
+    RET(launch_matvec_fused(ctx, ctx->work_e, ctx->work_e2, 0));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int q = 0; q < 3; ++q) RET(launch_matvec_fused(ctx, ctx->work_e, ctx->work_e2, 0));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (ms < best) {
+      best = ms;
+      bestZ = depths[a];
+    }
+  }
+  set_grids_fused(ctx->meta, bestZ);
+  ctx->tunedF = true;
+  ctx->cg_graph_check = -1;
+  CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PYIB_OK;
+}
+
 // Autotuner: time the float64 matvec for every pair of z-chunk depths (cells, nodes)
 // and keep the fastest.  Runs once per context, before any CG graph is captured.
 int tune_matvec(pyib_ctx* ctx) {
@@ -2019,14 +2633,23 @@ int set_state_solver(pyib_ctx* ctx, double dt, int alpd) {
 }
 
 int masked_matvec(pyib_ctx* ctx, const double* in, double* out, double dt, int alpd) {
-  RET(set_state_solver(ctx, dt, alpd));
+  RET(set_state_solver(ctx, dt, alpd & 1));
+  if (alpd & 2) {
+    // the single-pass fused matvec (viscous block always on)
+    if (!(alpd & 1)) return set_err(ctx, PYIB_E_ARG, "the fused matvec needs the viscous block (alpd 3)");
+    if (!ctx->tunedF) set_grids_fused(ctx->meta, ctx->meta.kzF > 0 ? ctx->meta.kzF : 16);
+    return launch_matvec_fused(ctx, in, out, 0);
+  }
   RET(launch_matvec(ctx, in, out, alpd, 0));
   return PYIB_OK;
 }
 
 // one CG iteration (5 kernels)
 int cg_iteration(pyib_ctx* ctx) {
-  RET(launch_matvec(ctx, ctx->p, ctx->w, 1, 1));
+  if (ctx->use_fused)
+    RET(launch_matvec_fused(ctx, ctx->p, ctx->w, 1));
+  else
+    RET(launch_matvec(ctx, ctx->p, ctx->w, 1, 1));
   const long long ne = ctx->lay.nedge;
   const unsigned int* pb = tp<unsigned int>(ctx, PYIB_T_PREC_BITS);
   k_cg_update<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ctx->meta, ne, ctx->r, ctx->w, pb,
@@ -2081,6 +2704,7 @@ int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
   RET(tune_matvec(ctx));
+  if (ctx->use_fused) RET(tune_fused(ctx));
   RET(set_state_solver(ctx, dt, 1));
   RET(build_cg_graph(ctx));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -2735,6 +3359,11 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
     }
   }
   m.nc = cb; m.nf = fb; m.ne = eb;
+  set_grids_fused(m, 16);
+  {
+    const char* f = std::getenv("PYIB_FUSED_MATVEC");
+    ctx->use_fused = f && f[0] == '1';
+  }
   {
     // default z-chunk depth: the deepest of 16, 8, 4, 2, 1 planes that still yields
     // enough tiles (the autotuner may change it, see tune_matvec)
@@ -2805,7 +3434,8 @@ int pyib_destroy(pyib_ctx* ctx) {
                   ctx->ibcell, ctx->ibbase, ctx->sort_keys_in, ctx->sort_keys_out, ctx->sort_vals_in,
                   ctx->sort_vals_out, ctx->sort_tmp, ctx->x32, ctx->r32, ctx->p32, ctx->w32,
                   ctx->vcm32, ctx->vq32, ctx->prec32, ctx->pa_val32, ctx->pv_val32,
-                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->ibjac, ctx->ws, ctx->ws_tmp};
+                  ctx->pr_val32, ctx->diag1, ctx->diag2, ctx->ibjac, ctx->ws, ctx->ws_tmp,
+                  ctx->f_irrA, ctx->f_irrV, ctx->f_needR, ctx->f_list, ctx->f_flags};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
@@ -2856,6 +3486,8 @@ int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes) {
   ctx->diag_for_kfac = -1.0;
   ctx->tuned = false;
   ctx->tuned32 = false;
+  ctx->tunedF = false;
+  ctx->fused_ready = false;
   return PYIB_OK;
 }
 
@@ -2866,7 +3498,10 @@ int pyib_finalize(pyib_ctx* ctx, const int64_t* counts, int32_t ncounts) {
   ctx->nR = counts[2];
   ctx->meta.ri_up = (ncounts >= 4 && counts[3] != 0) ? 0 : 1;
   set_grids(ctx->meta, ctx->meta.kz, ctx->meta.kzR);
+  set_grids_fused(ctx->meta, ctx->meta.kzF > 0 ? ctx->meta.kzF : 16);
   ctx->tuned32 = false;
+  ctx->tunedF = false;
+  ctx->fused_ready = false;
   if ((long long)ctx->meta.gxR * ctx->meta.gyR * ctx->meta.gzR + patch_grid(ctx->nR) > kPartStride ||
       (long long)ctx->meta.nplanes + patch_grid(ctx->nR) > kPartStride)
     return set_err(ctx, PYIB_E_ARG, "too many reduction slots for this layout");
@@ -3400,6 +4035,72 @@ int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
   return bench_matvec_t<double>(ctx, reps, ctx->work_e, ctx->work_e2, ctx->vcm, ctx->vq,
                                 tp<double>(ctx, PYIB_T_PA_VAL), tp<double>(ctx, PYIB_T_PV_VAL),
                                 tp<double>(ctx, PYIB_T_PR_VAL), ms_per);
+}
+
+// The fused float64 matvec timed with CUDA events: ms_per[0] the whole matvec,
+// [1] the exact vc rows and listed template vc, [2] the exact vq rows, [3] k_mvF,
+// [4] the exact w rows with the final dot.
+int pyib_bench_matvec_fused(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per) {
+  if (!ctx || !ms_per || reps <= 0) return PYIB_E_ARG;
+  if (!tables_ready(ctx) || !ctx->have_params) return set_err(ctx, PYIB_E_STATE, "context not ready");
+  CK(cudaSetDevice(ctx->device));
+  RET(set_state_solver(ctx, dt, 1));
+  RET(tune_fused(ctx));
+  RET(set_state_solver(ctx, dt, 1));
+  const double* in = ctx->work_e;
+  double* out = ctx->work_e2;
+  RET(launch_matvec_fused(ctx, in, out, 1));   // warm
+  float ms = 0.f;
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  for (int q = 0; q < reps; ++q) RET(launch_matvec_fused(ctx, in, out, 1));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ms_per[0] = ms / reps;
+  const Meta& m = ctx->meta;
+  const long long nc = ctx->lay.ncell;
+  const FusedTabs tb{ctx->f_irrA, ctx->f_irrV, ctx->f_needR, tp<unsigned int>(ctx, PYIB_T_PR_BITS),
+                     ctx->f_flags};
+  for (int kern = 0; kern < 4; ++kern) {
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int q = 0; q < reps; ++q) {
+      if (kern == 0) {
+        if (ctx->nA > 0) {
+          k_patchA<double><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
+              ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR),
+              tp<int>(ctx, PYIB_T_PA_COL), tp<double>(ctx, PYIB_T_PA_VAL), in, ctx->vcm, nc, ctx->st);
+          CKL();
+        }
+        if (ctx->n_list > 0) {
+          k_vc_list<<<patch_grid(ctx->n_list), kThreads, 0, ctx->stream>>>(m, ctx->n_list, ctx->f_list, in,
+                                                                            ctx->vcm, ctx->st);
+          CKL();
+        }
+      } else if (kern == 1) {
+        if (ctx->nV > 0) {
+          k_patchV<double><<<patch_grid(ctx->nV), kThreads, 0, ctx->stream>>>(
+              ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR),
+              tp<int>(ctx, PYIB_T_PV_COL), tp<double>(ctx, PYIB_T_PV_VAL), ctx->vcm, ctx->vq, nc, ctx->st);
+          CKL();
+        }
+      } else if (kern == 2) {
+        k_mvF<<<dim3(m.gxF, m.gyF, m.gzF), dim3(FX, FY, 1), kFusedSmemBytes, ctx->stream>>>(m, in, out, ctx->vcm, ctx->vq, tb,
+                                                                             ctx->partials, ctx->st, 1);
+        CKL();
+      } else {
+        k_patchRI<double><<<patch_grid(ctx->nR), kThreads, 0, ctx->stream>>>(
+            ctx->nR, tp<int>(ctx, PYIB_T_PR_IDS), tp<long long>(ctx, PYIB_T_PR_PTR), tp<int>(ctx, PYIB_T_PR_COL),
+            tp<double>(ctx, PYIB_T_PR_VAL), ctx->vq, out, in, ctx->partials, m.nplanesF, ctx->st, 1);
+        CKL();
+      }
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ms_per[1 + kern] = ms / reps;
+  }
+  ms_per[5] = (double)m.kzF;
+  return PYIB_OK;
 }
 
 }  // extern "C"

@@ -174,7 +174,9 @@ int pyib_get_field(pyib_ctx* ctx, int32_t field, void* host, size_t count);
 /* ---- operators (tests and the Python driver) ------------------------------ */
 /* w = (R I V P C) p with Dirichlet/absent rows zeroed: IBCore.flow_mat +
  * DirBC (ib_core_np.py:168-175, ib_driver_np.py:29-33) / Asp @ pp
- * (ib_driver_np.py:387).  alpd != 0 selects the viscous block. */
+ * (ib_driver_np.py:387).  alpd 1 selects the viscous block (0: without it);
+ * alpd 3 computes the same product (viscous block on) with the single-pass fused
+ * kernel the float64 CG uses, whose rows are bit-identical to the three-kernel path. */
 int pyib_matvec(pyib_ctx* ctx, int32_t in_field, int32_t out_field, double dt, int32_t alpd);
 /* Single-component operators on the scratch fields:
  *  op 0: curl   WORK_E  -> WORK_F  (ib_core_np.py:133)
@@ -264,6 +266,13 @@ int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms);
  * dot, [6] its patch rows with the final reduction.  With params.precision = 1 the
  * float32 matvec of the mixed solver is timed instead (on a float32 copy of WORK_E). */
 int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
+
+/* The single-pass float64 matvec of the CG (k_mvF with its exact-row kernels),
+ * timed with CUDA events over reps calls on WORK_E: ms_per[0] the whole matvec,
+ * [1] exact vc rows plus the listed template vc, [2] exact vq rows, [3] k_mvF,
+ * [4] exact w rows with the final dot; ms_per[5] = the tuned node planes per block.
+ * Counterpart: the operator timed is Asp @ pp / IBCore.flow_mat (ib_driver_np.py:387). */
+int pyib_bench_matvec_fused(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
 
 /* Deterministic spreading that allocates nothing.  No counterpart in the reference.
  *

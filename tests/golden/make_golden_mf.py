@@ -1,6 +1,10 @@
 """Trajectory goldens from the reference's matrix-free path (``solver.sparse = false``).
 
-    PYIB_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden_mf.py [case ...]
+    PYIB_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden_mf.py [case ...] [--out=PATH]
+
+    # the reference's own spread: the same case with one BLAS thread, then
+    OPENBLAS_NUM_THREADS=1 ... make_golden_mf.py CASE --out=/tmp/CASE_blas1.npz
+    python tests/golden/add_self_spread.py CASE /tmp/CASE_blas1.npz
 
 The reference's ``sparse = false`` path applies the Helmholtz operator with
 ``IBCore.flow_mat`` (``ib_core_np.py:168-175``) instead of its assembled CSR
@@ -117,7 +121,7 @@ def to_dense_cell3(v, pc):
     return out
 
 
-def generate(name, h, hws, kw, steps, progress_dir=None):
+def generate(name, h, hws, kw, steps, progress_dir=None, out_path=None):
     R.import_reference()
     case = R.RefCase(h, hws, sparse=False, **kw)
     core, drv = case.core, case.driver
@@ -177,7 +181,7 @@ def generate(name, h, hws, kw, steps, progress_dir=None):
     params = dict(h=h, half_widths=list(hws), steps=steps, sparse=False,
                   **{k: (list(v) if isinstance(v, tuple) else v) for k, v in kw.items()})
     out["params_json"] = np.bytes_(json.dumps(params))
-    np.savez_compressed(HERE / f"{name}.npz", **out)
+    np.savez_compressed(Path(out_path) if out_path else HERE / f"{name}.npz", **out)
     print(name, "done", "iters per step", [int(r[1]) for r in hist], f"{time.time() - t0:.0f}s", flush=True)
 
 
@@ -197,9 +201,11 @@ def _run(case, steps, cb, solves):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    prog = None
+    prog = out = None
     for a in sys.argv[1:]:
         if a.startswith("--progress="):
             prog = a.split("=", 1)[1]
+        if a.startswith("--out="):
+            out = a.split("=", 1)[1]
     for n in args or list(CASES):
-        generate(n, *CASES[n], progress_dir=prog)
+        generate(n, *CASES[n], progress_dir=prog, out_path=out)

@@ -8,8 +8,11 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def test_reference_arm_prints_its_line():
-    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=str(ROOT))
+    """The reference arm on the D = 8 layout of the benchmark geometry (the default
+    D = 32 arm builds the oracle on 5.8 M cells, minutes and about 19 GB of host memory)."""
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload",
+                          "d8_oscillating_sphere", "--steps", "1", "--warmup", "3"],
+                         capture_output=True, text=True, timeout=600, cwd=str(ROOT))
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
@@ -18,6 +21,10 @@ def test_reference_arm_prints_its_line():
         assert key in line, key
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    # full layout of the workload, real iterations, the extrapolation labelled
+    assert line["config"]["workload"] == "d8_oscillating_sphere" and line["config"]["cells"] == 90_112
+    assert line["extrapolated"] is True and line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["value_one_blas_thread"] > 0 and line["cpu_baseline"]["cpu_model"]
 
 
 def test_pressure_reference_arm_prints_its_line():
