@@ -555,6 +555,62 @@ def run_matvec(args):
     return 0
 
 
+def run_adjoint(args):
+    """Gradient of the first-harmonic axial force amplitude over the last period of
+    the adjoint configuration (D = 16, 2 levels, A = 0.2 D, Re0 = 1, 200 steps per
+    period, 804 markers; ``--adjoint-steps`` steps, default 400) with respect to A,
+    T and the marker positions, by the discrete adjoint with at most 20 stored
+    states, and central differences (step 1e-6 relative; 1e-6 h along seeded unit
+    marker directions) of the same float64 model for the quantities in
+    ``--adjoint-fd``.  The reference markers carry the seeded perturbation
+    0.01 h N(0, 1) of the configuration.  One JSON line; wall-clock seconds."""
+    import _pyib_b200_import
+    _pyib_b200_import.load()
+    import torch
+    from pyib_b200 import adjoint as AD
+    from pyib_b200 import build
+    from pyib_b200.cases import CASES
+    build.build_library()
+    case = CASES["d16_adjoint_sphere" if args.workload == "d32_oscillating_sphere" else args.workload]
+    steps = args.adjoint_steps
+    window = case.steps_per_period
+    model = AD.CavityModel(case, tol=args.adjoint_tol)
+    rng = np.random.default_rng(0)
+    ref = model.ref0 + torch.from_numpy(0.01 * model.h0 * rng.standard_normal(tuple(model.ref0.shape))).to(model.dev)
+    A, T = case.amplitude, case.period
+    t0 = time.perf_counter()
+    J, gA, gT, gref, info = AD.force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20)
+    t_grad = time.perf_counter() - t0
+    fd = {}
+    t0 = time.perf_counter()
+    eps = 1e-6
+    f = lambda a, tt, r: AD.force_amplitude(model, a, tt, r, steps, window)
+    for item in [x for x in args.adjoint_fd.split(",") if x]:
+        if item == "A":
+            fd["A"] = ((f(A * (1 + eps), T, ref) - f(A * (1 - eps), T, ref)) / (2 * eps * A), gA)
+        elif item == "T":
+            fd["T"] = ((f(A, T * (1 + eps), ref) - f(A, T * (1 - eps), ref)) / (2 * eps * T), gT)
+        elif item.startswith("dir"):
+            q = int(item[3:])
+            d = np.random.default_rng(100 + q).standard_normal(tuple(ref.shape))
+            d /= np.linalg.norm(d)
+            dt_ = torch.from_numpy(d).to(model.dev)
+            h = eps * model.h0
+            fd[item] = ((f(A, T, ref + h * dt_) - f(A, T, ref - h * dt_)) / (2 * h), float(np.sum(gref * d)))
+    t_fd = time.perf_counter() - t0
+    rel = {k: abs(v[1] - v[0]) / max(abs(v[0]), 1e-300) for k, v in fd.items()}
+    line = {"workload": case.name, "metric": "adjoint gradient of the force amplitude", "steps": steps,
+            "window_steps": window, "cells": int(model.lay.cell_active.sum()),
+            "markers": int(model.ref0.shape[0]), "J": J, "dJ_dA": gA, "dJ_dT": gT,
+            "dJ_dmarkers_norm": float(np.linalg.norm(gref)), "finite_differences": fd,
+            "relative_differences": rel, "max_stored_states": info["max_stored_states"],
+            "recomputed_steps": info["recomputed_steps"], "forward_cg_iterations": info["forward_cg_iterations"],
+            "total_cg_iterations": info["total_cg_iterations"], "cell_cg_iterations": info["cell_cg_iterations"],
+            "gradient_seconds": t_grad, "finite_difference_seconds": t_fd, "tolerance": args.adjoint_tol}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def mixed_leg(case, tables, args, steps_done, final):
     """The mixed form on the same case and start: steps/s over ``args.steps`` steps
     (CUDA events, after ``args.warmup`` steps) and, after the same total number of
@@ -941,6 +997,12 @@ def main():
     ap.add_argument("--harmonic", action="store_true",
                     help="run --periods oscillation periods in float64 and mixed and fit the force")
     ap.add_argument("--periods", type=int, default=6)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="gradient of the force amplitude by the discrete adjoint (workload d16_adjoint_sphere)")
+    ap.add_argument("--adjoint-steps", type=int, default=400)
+    ap.add_argument("--adjoint-fd", default="A,T,dir0",
+                    help="comma list of central-difference checks: A, T, dir0, dir1, ...")
+    ap.add_argument("--adjoint-tol", type=float, default=1e-13)
     ap.add_argument("--matvec-only", action="store_true",
                     help="time the standalone float64 matvecs (three-kernel and fused) on the workload's layout")
     ap.add_argument("--compare-precision", action="store_true",
@@ -959,6 +1021,8 @@ def main():
         return run_pressure(args, world, rank, local)
     if args.matvec_only:
         return run_matvec(args)
+    if args.adjoint:
+        return run_adjoint(args)
     if args.compare_precision:
         return run_precision_compare(args, world, rank, local)
     if args.harmonic:

@@ -143,5 +143,10 @@ D8_FIXED = SphereCase(name="d8_fixed_sphere", cells_per_diameter=8, half_widths_
                       reynolds=100.0, inflow=1.0, amplitude_d=0.0, cavity=False,
                       dt=0.5 * (D / 8) / 1.0, cg_max_iterations=1000)
 
+# The adjoint configuration: D = 16 cells, two levels (half widths 2D, 4D), A = 0.2 D,
+# Re0 = 1, 200 steps per period (804 markers); its gradient runs over 400 steps.
+D16_ADJOINT = SphereCase(name="d16_adjoint_sphere", cells_per_diameter=16, half_widths_d=(2.0, 4.0),
+                         reynolds=1.0, amplitude_d=0.2)
+
 CASES = {c.name: c for c in (D32_OSCILLATING, D40_OSCILLATING, D24_OSCILLATING, D16_OSCILLATING, D8_OSCILLATING,
-                               D8_FIXED)}
+                               D8_FIXED, D16_ADJOINT)}
