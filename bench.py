@@ -581,6 +581,7 @@ def run_adjoint(args):
     t0 = time.perf_counter()
     J, gA, gT, gref, info = AD.force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20)
     t_grad = time.perf_counter() - t0
+    print("# gradient", json.dumps({"J": J, "dJ_dA": gA, "dJ_dT": gT, "seconds": t_grad}), file=sys.stderr, flush=True)
     fd = {}
     t0 = time.perf_counter()
     eps = 1e-6
@@ -597,6 +598,7 @@ def run_adjoint(args):
             dt_ = torch.from_numpy(d).to(model.dev)
             h = eps * model.h0
             fd[item] = ((f(A, T, ref + h * dt_) - f(A, T, ref - h * dt_)) / (2 * h), float(np.sum(gref * d)))
+        print("# finite difference", item, fd[item], time.perf_counter() - t0, file=sys.stderr, flush=True)
     t_fd = time.perf_counter() - t0
     rel = {k: abs(v[1] - v[0]) / max(abs(v[0]), 1e-300) for k, v in fd.items()}
     line = {"workload": case.name, "metric": "adjoint gradient of the force amplitude", "steps": steps,
