@@ -16,14 +16,22 @@ Laplacian in CSR (rows sorted by neighbour and face), the connectivity check,
 the CG and the gauge, all with sums in fixed orders.  ``assemble`` builds the
 same reduced system on the host for callers of the generic CSR solver
 ``graph_pcg`` (``pyib_graph_pcg``).  There is no CPU solve: the calls fail if
-the library is missing.  The reference's band repair
-(``ib_postprocess.py:213-250``, an lsqr on the few cells next to the body) is
-not part of this module.
+the library is missing.
+
+``repair_pressure_band`` is the reference's band repair
+(``ib_postprocess.py:200-250``) on a ``UniformLattice`` (``ib_postprocess.py:108-140``):
+the least-squares fit of the band cells' pressure to the lattice-edge jumps,
+the cells outside the band held.  The reference solves it with ``lsqr``; here
+its normal equations (a graph Laplacian plus one diagonal term per edge to a
+held cell, positive definite once every band component is anchored) are
+solved by ``graph_pcg`` on the device to a tighter tolerance than lsqr's
+``atol = btol = 1e-11``, so both reach the same least-squares solution.
 """
 from __future__ import annotations
 
 import ctypes as C
 import threading
+from dataclasses import dataclass
 
 import numpy as np
 from scipy.sparse import csr_matrix
@@ -230,3 +238,147 @@ def recover_pressure(cell_positions, face_cells, face_area, gradient, *, toleran
         "iterations": int(info[1]),
     }
     return out, diagnostics
+
+
+@dataclass
+class UniformLattice:
+    """The finest uniform block of a saved snapshot (``ib_postprocess.py:108-140``):
+    global cell ids (-1 where the block has no cell), origin and spacing."""
+
+    cell_ids: np.ndarray
+    origin: np.ndarray
+    spacing: float
+
+    def __post_init__(self):
+        self.cell_ids = np.asarray(self.cell_ids)
+        self.origin = _finite("lattice_origin", self.origin, (3,))
+        self.spacing = float(self.spacing)
+        if self.cell_ids.ndim != 3 or self.cell_ids.dtype.kind not in "iu":
+            raise ValueError("index_cell must be a 3D integer array")
+        if min(self.cell_ids.shape) < 2 or not np.isfinite(self.spacing) or self.spacing <= 0:
+            raise ValueError("the lattice needs at least two cells per axis and positive spacing")
+
+    @property
+    def shape(self):
+        return self.cell_ids.shape
+
+    def coordinates(self):
+        return self.origin + self.spacing * np.indices(self.shape).transpose(1, 2, 3, 0)
+
+    def field(self, cell_field):
+        """A per-cell field gathered onto the lattice (NaN where there is no cell)."""
+        cell_field = np.asarray(cell_field)
+        valid = self.cell_ids >= 0
+        out = np.full(self.shape + cell_field.shape[1:], np.nan)
+        out[valid] = cell_field[self.cell_ids[valid]]
+        return out
+
+
+def lattice_edges(shape, valid):
+    """Axis-neighbour pairs of a lattice with both cells valid, x edges first, then
+    y, then z, each in C order of the lower cell (``ib_postprocess.py:200-210``):
+    (first, second, axis)."""
+    ids = np.arange(int(np.prod(shape)), dtype=np.int64).reshape(shape)
+    vflat = np.asarray(valid).ravel()
+    parts = []
+    for axis in range(3):
+        lo, hi = [slice(None)] * 3, [slice(None)] * 3
+        lo[axis], hi[axis] = slice(None, -1), slice(1, None)
+        a, b = ids[tuple(lo)].ravel(), ids[tuple(hi)].ravel()
+        keep = vflat[a] & vflat[b]
+        parts.append((a[keep], b[keep], np.full(int(keep.sum()), axis, dtype=np.int64)))
+    return tuple(np.concatenate([p[k] for p in parts]) for k in range(3))
+
+
+def band_system(shape, spacing, raw_pressure, regular_gradient, signed_distance, width=1.5):
+    """The band repair's least-squares problem and its normal equations, on the host.
+
+    Band (target) cells: valid (signed distance >= 0, finite raw pressure) within
+    ``width * spacing`` of the surface.  Every valid edge touching the band asks
+    ``p[second] - p[first] = spacing (g[first] + g[second])_axis / 2``; a cell outside
+    the band keeps its raw value, moved to the right-hand side.  Returns
+    ``(target, ids, ptr, col, val, rhs)``: the mask, the band's flat lattice ids,
+    and the CSR and right-hand side of ``B^T B x = B^T r``.  Raises the reference's
+    ValueErrors for an empty or an unanchored band.
+    """
+    raw = np.asarray(raw_pressure, dtype=np.float64)
+    dist = np.asarray(signed_distance, dtype=np.float64)
+    grad = np.asarray(regular_gradient, dtype=np.float64)
+    if raw.shape != tuple(shape) or dist.shape != tuple(shape) or grad.shape != tuple(shape) + (3,):
+        raise ValueError("band repair fields must match the lattice shape")
+    with np.errstate(invalid="ignore"):
+        valid = (dist >= 0) & np.isfinite(raw)
+        target = valid & (dist <= width * spacing)
+    first, second, axes = lattice_edges(shape, valid)
+    tflat = target.ravel()
+    sel = tflat[first] | tflat[second]
+    first, second, axes = first[sel], second[sel], axes[sel]
+    ids = np.flatnonzero(tflat)
+    n = len(ids)
+    if not n:
+        raise ValueError("pressure repair band contains no cells; refine the grid")
+    local = np.full(tflat.size, -1, dtype=np.int64)
+    local[ids] = np.arange(n)
+    g = grad.reshape(-1, 3)
+    r = 0.5 * spacing * (g[first, axes] + g[second, axes])
+    rflat = raw.ravel()
+    la, lb = local[first], local[second]
+    both = (la >= 0) & (lb >= 0)
+    only_a = (la >= 0) & (lb < 0)        # second cell held: p[a] = raw[b] - r
+    only_b = (la < 0) & (lb >= 0)        # first cell held: p[b] = raw[a] + r
+    # anchored components: every connected piece of the band needs a held neighbour
+    count, labels = connected_components(
+        csr_matrix((np.ones(int(both.sum())), (la[both], lb[both])), shape=(n, n)), directed=False)
+    anchored = np.zeros(count, dtype=bool)
+    anchored[labels[la[only_a]]] = True
+    anchored[labels[lb[only_b]]] = True
+    if not anchored.all():
+        raise ValueError("pressure repair has an unanchored band; enlarge the finest region")
+    # normal equations: B^T B (Laplacian of band-band edges, +1 on the diagonal per
+    # held neighbour) and B^T r (r with the held values moved over)
+    rows = np.concatenate([la[both], lb[both], la[both], lb[both], la[only_a], lb[only_b]])
+    cols = np.concatenate([lb[both], la[both], la[both], lb[both], la[only_a], lb[only_b]])
+    m = int(both.sum())
+    vals = np.concatenate([-np.ones(2 * m), np.ones(2 * m), np.ones(int(only_a.sum()) + int(only_b.sum()))])
+    key = rows * n + cols
+    order = np.argsort(key, kind="stable")
+    key, vals = key[order], vals[order]
+    start = np.flatnonzero(np.r_[True, key[1:] != key[:-1]])
+    val = np.add.reduceat(vals, start)
+    ukey = key[start]
+    ptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(ukey // n, minlength=n), out=ptr[1:])
+    col = (ukey % n).astype(np.int32)
+    rhs = (np.bincount(lb[both], r[both], minlength=n) - np.bincount(la[both], r[both], minlength=n)
+           + np.bincount(la[only_a], rflat[second[only_a]] - r[only_a], minlength=n)
+           + np.bincount(lb[only_b], rflat[first[only_b]] + r[only_b], minlength=n))
+    return target, ids, ptr, col, val, rhs
+
+
+def repair_pressure_band(lattice, raw_pressure, regular_gradient, signed_distance, *, width=1.5,
+                         tolerance=1e-13, handle=None, device=0, timing=None):
+    """The reference's band repair (``ib_postprocess.py:213-250``): the band cells'
+    pressure refitted in the least-squares sense to the gradient jumps, every other
+    cell returned unchanged.
+
+    Same arguments, result ``(repaired, target, iterations)`` and errors as the
+    reference (ValueError for an empty or unanchored band, RuntimeError when the
+    solve fails).  ``iterations`` counts the device CG's iterations on the normal
+    equations (the reference reports lsqr's).  ``lattice`` needs ``shape`` and
+    ``spacing`` (a ``UniformLattice``).  The solve stops at
+    ``|r| < tolerance |b|``, with at most ``max(500, 20 n)`` iterations as the
+    reference's lsqr.
+    """
+    shape = tuple(lattice.shape)
+    target, ids, ptr, col, val, rhs = band_system(shape, float(lattice.spacing), raw_pressure,
+                                                  regular_gradient, signed_distance, width)
+    h = default_handle(device) if handle is None else handle
+    try:
+        x, iterations = graph_pcg(h, ptr, col, val, rhs, tolerance, max(500, 20 * len(ids)), timing)
+    except _lib.B200Error as e:
+        raise RuntimeError(f"pressure band solve failed ({e})") from e
+    if not np.isfinite(x).all():
+        raise RuntimeError("pressure band solve failed (non-finite result)")
+    repaired = np.asarray(raw_pressure, dtype=np.float64).ravel().copy()
+    repaired[ids] = x
+    return repaired.reshape(shape), target, iterations

@@ -11,17 +11,24 @@ the Laplacian ``B^T W B`` reduced by pinning cell 0 (rows and columns 1..n-1),
 ``atol = 0``, ``maxiter = max(2000, 10 n)``, then the boundary-adjacent mean
 removed (``ib_postprocess.py:99-102``).
 
-Parity pin: ``tests/test_pressure_oracle.py`` checks this restatement against
-``tests/golden/pressure_n2_mesh.npz``, made by running the reference's own
-function (``tests/golden/make_pressure_golden.py``), and against the
-reference's quadratic known-answer case (``tests/test_ib_postprocess.py:76-84``).
+Also restates the band repair ``repair_pressure_band``
+(``ib_postprocess.py:200-250``): the lattice edges between valid cells, the
+edges touching the band, their jumps, the incidence with the values of the
+cells outside the band moved to the right-hand side, the anchor check, and
+``scipy.sparse.linalg.lsqr`` with ``atol = btol = 1e-11``.
+
+Parity pin: ``tests/test_pressure_oracle.py`` checks these restatements against
+``tests/golden/pressure_golden.npz`` and ``tests/golden/band_golden.npz``, made by
+running the reference's own functions (``tests/golden/make_pressure_golden.py``,
+``tests/golden/make_band_golden.py``), and against the reference's known-answer
+cases (``tests/test_ib_postprocess.py:76-84, 86-95``).
 """
 from __future__ import annotations
 
 import numpy as np
 from scipy.sparse import coo_matrix, diags
 from scipy.sparse.csgraph import connected_components
-from scipy.sparse.linalg import cg
+from scipy.sparse.linalg import cg, lsqr
 
 
 def recover_pressure_checked(cell_positions, face_cells, face_area, gradient, *, tolerance=1e-10):
@@ -126,3 +133,87 @@ def quadratic_gradient(points):
     """Its gradient (``tests/test_ib_postprocess.py:49-51``)."""
     x, y, z = np.asarray(points).T
     return np.column_stack((0.2 + 0.8 * x + 0.1 * y, -0.5 - 0.4 * y + 0.1 * x, 0.7 + 0.6 * z))
+
+
+def lattice_edges(shape, valid):
+    """Edges between axis neighbours that are both valid, axis by axis
+    (``ib_postprocess.py:200-210``): first cell, second cell, axis."""
+    ids = np.arange(int(np.prod(shape))).reshape(shape)
+    out = [[], [], []]
+    for axis in range(3):
+        lo, hi = [slice(None)] * 3, [slice(None)] * 3
+        lo[axis], hi[axis] = slice(None, -1), slice(1, None)
+        a, b = ids[tuple(lo)].ravel(), ids[tuple(hi)].ravel()
+        keep = valid.ravel()[a] & valid.ravel()[b]
+        out[0].append(a[keep])
+        out[1].append(b[keep])
+        out[2].append(np.full(int(keep.sum()), axis))
+    return tuple(np.concatenate(v) for v in out)
+
+
+def repair_pressure_band(shape, spacing, raw_pressure, regular_gradient, signed_distance, width=1.5):
+    """The reference's band repair (``ib_postprocess.py:213-250``); returns
+    (repaired, target, lsqr iterations)."""
+    target = (signed_distance >= 0) & (signed_distance <= width * spacing) & np.isfinite(raw_pressure)
+    valid = (signed_distance >= 0) & np.isfinite(raw_pressure)
+    first, second, axes = lattice_edges(shape, valid)
+    sel = target.ravel()[first] | target.ravel()[second]
+    first, second, axes = first[sel], second[sel], axes[sel]
+    ids = np.flatnonzero(target.ravel())
+    if not len(ids):
+        raise ValueError("pressure repair band contains no cells; refine the grid")
+    local = np.full(target.size, -1)
+    local[ids] = np.arange(len(ids))
+    g = regular_gradient.reshape(-1, 3)
+    rhs = 0.5 * spacing * (g[first, axes] + g[second, axes])
+    raw = raw_pressure.ravel()
+    rows, cols, vals = [], [], []
+    for sign, cells in ((-1.0, first), (1.0, second)):
+        inside = local[cells] >= 0
+        rows.append(np.flatnonzero(inside))
+        cols.append(local[cells[inside]])
+        vals.append(np.full(int(inside.sum()), sign))
+        rhs[~inside] -= sign * raw[cells[~inside]]
+    B = coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                   shape=(len(first), len(ids))).tocsr()
+    count, labels = connected_components((B.T @ B).tocsr(), directed=False)
+    anchors = np.zeros(len(ids), dtype=bool)
+    for a, b in ((first, second), (second, first)):
+        hit = (local[a] >= 0) & (local[b] < 0)
+        anchors[local[a[hit]]] = True
+    if len(np.unique(labels[anchors])) != count:
+        raise ValueError("pressure repair has an unanchored band; enlarge the finest region")
+    sol = lsqr(B, rhs, atol=1e-11, btol=1e-11, iter_lim=max(500, 20 * len(ids)))
+    if sol[1] not in (0, 1, 2, 4, 5) or not np.isfinite(sol[0]).all():
+        raise RuntimeError(f"pressure band solve failed (status {sol[1]})")
+    out = raw.copy()
+    out[ids] = sol[0]
+    return out.reshape(shape), target, int(sol[2])
+
+
+def band_case(count=17, spacing=0.25, radius=0.6, noise=0.0, seed=0, holes=0.0):
+    """Lattice inputs of the reference's band test (``tests/test_ib_postprocess.py:86-95``):
+    a count^3 block centred on the origin, the signed distance to a sphere of
+    ``radius``, the quadratic truth, a raw pressure with the defect
+    ``0.8 cos(x)`` on the band, and the quadratic's gradient; ``noise`` adds a
+    seeded normal perturbation to the gradient so that the band's equations are
+    inconsistent, and ``holes`` sets that fraction of the raw values (seeded)
+    to NaN, cells the repair must leave out.  Returns (positions, distance,
+    truth, raw, gradient), the
+    lattice arrays shaped (count, count, count[, 3])."""
+    shape = (count,) * 3
+    axes = (np.arange(count) - 0.5 * (count - 1)) * spacing
+    pos = np.stack(np.meshgrid(axes, axes, axes, indexing="ij"), axis=-1)
+    flat = pos.reshape(-1, 3)
+    distance = (np.linalg.norm(flat, axis=1) - radius).reshape(shape)
+    truth = quadratic(flat).reshape(shape)
+    band = (distance >= 0) & (distance <= 1.5 * spacing)
+    raw = truth.copy()
+    raw[band] += 0.8 * np.cos(pos[band, 0])
+    grad = quadratic_gradient(flat)
+    rng = np.random.default_rng(seed)
+    if noise:
+        grad = grad + noise * rng.standard_normal(grad.shape)
+    if holes:
+        raw[rng.random(shape) < holes] = np.nan
+    return pos, distance, truth, raw, grad.reshape(shape + (3,))

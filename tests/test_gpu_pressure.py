@@ -197,3 +197,56 @@ def test_edge_cases_match_oracle():
     assert d["gauge"] == e["gauge"] == "mean cells = 0"
     assert abs(p.mean()) < 1e-14
     assert np.max(np.abs(p - q)) <= 1e-9 * np.max(np.abs(q))
+
+
+# ---- band repair on the device (ib_postprocess.py:213-250) -------------------
+BAND = np.load(PU.GOLDEN / "band_golden.npz")
+BAND_CASES = {
+    "q17": dict(count=17, spacing=0.25, width=1.5),
+    "n40w15": dict(count=40, spacing=1.0 / 16, width=1.5, noise=0.05, seed=7, holes=0.02),
+    "n40w25": dict(count=40, spacing=1.0 / 16, width=2.5, noise=0.05, seed=7, holes=0.02),
+}
+
+
+def _band(name):
+    c = BAND_CASES[name]
+    kw = {k: c[k] for k in ("noise", "seed", "holes") if k in c}
+    _, dist, truth, raw, grad = PO.band_case(c["count"], c["spacing"], **kw)
+    ids = np.arange(c["count"] ** 3).reshape((c["count"],) * 3)
+    lat = PP.UniformLattice(ids, np.full(3, -0.5 * (c["count"] - 1) * c["spacing"]), c["spacing"])
+    return c, lat, dist, truth, raw, grad
+
+
+@pytest.mark.parametrize("name", sorted(BAND_CASES))
+def test_band_repair_matches_reference(name):
+    """The device CG on the normal equations reaches the reference's lsqr answer
+    to lsqr's own stopping error (1e-9 of the pressure range); cells outside the
+    band are returned bit for bit."""
+    c, lat, dist, _, raw, grad = _band(name)
+    rep, target, it = PP.repair_pressure_band(lat, raw, grad, dist, width=c["width"])
+    np.testing.assert_array_equal(target, BAND[f"{name}_target"])
+    want = BAND[f"{name}_values"]
+    assert np.max(np.abs(rep[target] - want)) <= 1e-9 * np.max(np.abs(want))
+    keep = ~target & np.isfinite(raw)
+    np.testing.assert_array_equal(rep[keep], raw[keep])
+    np.testing.assert_array_equal(np.isnan(rep), np.isnan(raw) & ~target)
+    assert 0 < it <= max(500, 20 * int(target.sum()))
+    rep2, _, it2 = PP.repair_pressure_band(lat, raw, grad, dist, width=c["width"])
+    np.testing.assert_array_equal(rep, rep2)
+    assert it2 == it
+
+
+def test_band_repair_known_answer():
+    """The reference's own case and bound (tests/test_ib_postprocess.py:86-95)."""
+    c, lat, dist, truth, raw, grad = _band("q17")
+    rep, target, _ = PP.repair_pressure_band(lat, raw, grad, dist)
+    np.testing.assert_allclose(rep[target], truth[target], atol=1e-9, rtol=1e-9)
+    np.testing.assert_array_equal(rep[~target], raw[~target])
+
+
+@pytest.mark.parametrize("key,shift,width", [("unanchored", 0.0, 100.0), ("empty", 10.0, 1.5)])
+def test_band_repair_rejections(key, shift, width):
+    c, lat, dist, _, raw, grad = _band("q17")
+    with pytest.raises(ValueError) as e:
+        PP.repair_pressure_band(lat, raw, grad, dist + shift, width=width)
+    assert str(e.value) == str(BAND[f"{key}_message"])

@@ -90,3 +90,89 @@ def test_oracle_rejects_disconnected_graph():
             np.zeros((3, 3)))
     with pytest.raises(ValueError, match="disconnected"):
         PO.recover_pressure(*args)
+
+
+# ---- band repair (ib_postprocess.py:200-250) ---------------------------------
+BAND = np.load(PU.GOLDEN / "band_golden.npz")
+BAND_CASES = {
+    "q17": dict(count=17, spacing=0.25, width=1.5),
+    "n40w15": dict(count=40, spacing=1.0 / 16, width=1.5, noise=0.05, seed=7, holes=0.02),
+    "n40w25": dict(count=40, spacing=1.0 / 16, width=2.5, noise=0.05, seed=7, holes=0.02),
+}
+
+
+def band_inputs(name):
+    c = BAND_CASES[name]
+    kw = {k: c[k] for k in ("noise", "seed", "holes") if k in c}
+    _, dist, truth, raw, grad = PO.band_case(c["count"], c["spacing"], **kw)
+    return c, dist, truth, raw, grad
+
+
+@pytest.mark.parametrize("name", sorted(BAND_CASES))
+def test_band_oracle_matches_reference(name):
+    """The restated lsqr repair reproduces the reference's output and iteration count."""
+    c, dist, _, raw, grad = band_inputs(name)
+    rep, target, it = PO.repair_pressure_band(dist.shape, c["spacing"], raw, grad, dist, c["width"])
+    np.testing.assert_array_equal(target, BAND[f"{name}_target"])
+    assert np.max(np.abs(rep[target] - BAND[f"{name}_values"])) <= 1e-13 * np.max(np.abs(BAND[f"{name}_values"]))
+    assert it == int(BAND[f"{name}_iterations"])
+    np.testing.assert_array_equal(np.isnan(rep[~target]), np.isnan(raw[~target]))
+    keep = ~target & np.isfinite(raw)
+    np.testing.assert_array_equal(rep[keep], raw[keep])
+
+
+def test_band_oracle_known_answer():
+    """The reference's own bound (tests/test_ib_postprocess.py:86-95)."""
+    c, dist, truth, raw, grad = band_inputs("q17")
+    rep, target, _ = PO.repair_pressure_band(dist.shape, c["spacing"], raw, grad, dist)
+    np.testing.assert_allclose(rep[target], truth[target], atol=1e-9, rtol=1e-9)
+    np.testing.assert_array_equal(rep[~target], raw[~target])
+
+
+@pytest.mark.parametrize("name", sorted(BAND_CASES))
+def test_band_normal_equations_give_the_reference_solution(name):
+    """The product's host system (``band_system``): the same band, a symmetric
+    matrix, and -- solved exactly here -- the reference's least-squares answer to
+    within lsqr's own stopping error (1e-9 of the pressure range)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.linalg import spsolve
+    c, dist, _, raw, grad = band_inputs(name)
+    target, ids, ptr, col, val, rhs = PP.band_system(dist.shape, c["spacing"], raw, grad, dist, c["width"])
+    np.testing.assert_array_equal(target, BAND[f"{name}_target"])
+    np.testing.assert_array_equal(ids, np.flatnonzero(target.ravel()))
+    A = csr_matrix((val, col, ptr), shape=(len(ids), len(ids)))
+    assert abs(A - A.T).max() == 0.0
+    assert np.all(np.diff(col[ptr[0]:ptr[1]]) > 0)
+    x = spsolve(A.tocsc(), rhs)
+    want = BAND[f"{name}_values"]
+    assert np.max(np.abs(x - want)) <= 1e-9 * np.max(np.abs(want))
+
+
+def test_band_lattice_edges_follow_the_reference_order():
+    c, dist, _, raw, _ = band_inputs("n40w15")
+    valid = (dist >= 0) & np.isfinite(raw)
+    for a, b in zip(PP.lattice_edges(dist.shape, valid), PO.lattice_edges(dist.shape, valid)):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("key,shift,width", [("unanchored", 0.0, 100.0), ("empty", 10.0, 1.5)])
+def test_band_rejections_as_the_reference(key, shift, width):
+    c, dist, _, raw, grad = band_inputs("q17")
+    msg = str(BAND[f"{key}_message"])
+    with pytest.raises(ValueError, match=msg.split(";")[0]):
+        PO.repair_pressure_band(dist.shape, 0.25, raw, grad, dist + shift, width)
+    with pytest.raises(ValueError, match=msg.split(";")[0]):
+        PP.band_system(dist.shape, 0.25, raw, grad, dist + shift, width)
+
+
+def test_uniform_lattice_checks_and_field():
+    with pytest.raises(ValueError, match="3D integer"):
+        PP.UniformLattice(np.zeros((3, 3)), np.zeros(3), 0.1)
+    with pytest.raises(ValueError, match="at least two cells"):
+        PP.UniformLattice(np.zeros((1, 3, 3), dtype=int), np.zeros(3), 0.1)
+    ids = np.arange(27).reshape(3, 3, 3)
+    ids[0, 0, 0] = -1
+    lat = PP.UniformLattice(ids, np.array([1.0, 2.0, 3.0]), 0.5)
+    np.testing.assert_array_equal(lat.coordinates()[2, 1, 0], [2.0, 2.5, 3.0])
+    f = lat.field(np.arange(27.0))
+    assert np.isnan(f[0, 0, 0]) and f[2, 2, 2] == 26.0
