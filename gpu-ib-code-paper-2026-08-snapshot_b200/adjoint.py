@@ -32,8 +32,10 @@ marker positions.  The physical viscosity, density and time step are held at
 their nominal values: A and T enter through the prescribed motion, its
 velocity, the interior-momentum indicator's centre and the harmonic fit.
 
-``CavityModel(case, device="cpu")`` is a checking mode for tests without a GPU:
-the same model with a NumPy PCG of the device's recurrence and NumPy spreading.
+Every solve, product and spreading runs on the device through the library;
+without it ``CavityModel`` fails on construction.  (The CPU tests check the
+same model with a NumPy mirror of the device PCG and of the spreading, a
+subclass that lives with the tests.)
 """
 from __future__ import annotations
 
@@ -136,16 +138,13 @@ class HelmSolve(torch.autograd.Function):
 
 
 def _spread(model, cells32, w, ds3, f):
-    """out (NC, 3) = sum over contributions of f[m] * w * ds3[m]: the library's sort-and-sum."""
+    """out (NC, 3) = sum over contributions of f[m] * w * ds3[m] (``model.spread``)."""
+    return model.spread(cells32, w, ds3, f)
+
+
+def _spread_device(model, cells32, w, ds3, f):
+    """The library's deterministic sort-and-sum spreading (``pyib_spread_noalloc``)."""
     M = f.shape[0]
-    if model.solver is None:
-        # checking mode: the same sum with NumPy's bincount (in (marker, offset) order)
-        c = cells32.cpu().numpy()
-        ww = (w * ds3[:, None]).cpu().numpy().reshape(-1)
-        fm = f.detach().cpu().numpy()
-        out = np.stack([np.bincount(c, weights=np.repeat(fm[:, q], 125) * ww, minlength=model.NC)
-                        for q in range(3)], axis=1)
-        return torch.from_numpy(out)
     out = torch.empty(3 * model.NC, dtype=torch.float64, device=f.device)
     fm = f.contiguous().reshape(-1)
     wm = w.contiguous().reshape(-1)
@@ -253,7 +252,7 @@ class CavityModel:
     oscillation); ``tol`` is the PCG's mixed stopping tolerance (tol1, and tol2
     unless given), tighter than the reference's 1e-10 / 1e-9 so that finite
     differences of the objective resolve the gradient.  ``device`` is a CUDA
-    ordinal, or ``"cpu"`` for the checking mode.
+    ordinal.
     """
 
     def __init__(self, case, *, device=0, tol=1e-13, tol2=None, cg_max_iterations=200000):
@@ -268,23 +267,7 @@ class CavityModel:
         self.ac = self.ad = 0.5
         self.tol1, self.tol2 = float(tol), float(tol if tol2 is None else tol2)
         self.cg_max = int(cg_max_iterations)
-        if device == "cpu":
-            from .operators import Operators
-            self.dev = torch.device("cpu")
-            self.solver = None
-            ops = Operators(lay)
-            prec = ops.prec(ops.dir_mask(True))
-            A = ops.R @ sum(ops.I[q] @ ops.V(self.rou, self.visc, self.dt) @ ops.P[q] for q in range(3)) @ ops.C
-            self._free_idx = np.nonzero(prec != 0.0)[0]
-            self._Aff = A.tocsr()[self._free_idx][:, self._free_idx]
-            self._prec_f = prec[self._free_idx]
-        else:
-            self.dev = torch.device("cuda", device)
-            self.solver = DeviceSolver(lay, rou=self.rou, visc=self.visc, cavity=True, tol1=self.tol1,
-                                       tol2=self.tol2, cg_max_iterations=self.cg_max, device=device)
-            self.lib = _lib.load()
-            ops = self.solver.ops
-            prec = self.solver.prec
+        ops, prec = self._setup_solver(device)
         d = self.dev
         step_operators(lay, ops, self.visc, d, into=self)
         self.free = torch.from_numpy((prec != 0.0).astype(np.float64)).to(d)
@@ -323,37 +306,22 @@ class CavityModel:
         self.cell_iterations = 0
 
     # ---- solves ---------------------------------------------------------------------
+    def _setup_solver(self, device):
+        """The device context of the case's layout; returns (operators, preconditioner)."""
+        self.dev = torch.device("cuda", device)
+        self.solver = DeviceSolver(self.lay, rou=self.rou, visc=self.visc, cavity=True, tol1=self.tol1,
+                                   tol2=self.tol2, cg_max_iterations=self.cg_max, device=device)
+        self.lib = _lib.load()
+        return self.solver.ops, self.solver.prec
+
     def cells32(self, cells):
         return cells.to(torch.int32).contiguous().reshape(-1)
 
+    def spread(self, cells32, w, ds3, f):
+        return _spread_device(self, cells32, w, ds3, f)
+
     def solve(self, res_e, s):
-        """helm_solve: s + A+ res on the free edges (device PCG, or its NumPy mirror)."""
-        if self.solver is None:
-            # the device's PCG recurrence and mixed stopping test (ib_driver_np.py:331-403),
-            # tested every iteration
-            x = s.detach().cpu().numpy().copy()
-            xf = x[self._free_idx]
-            r = res_e.detach().cpu().numpy()[self._free_idx].copy()
-            mdiag = self._prec_f
-            y = np.zeros_like(r)
-            z = r * mdiag
-            p = z.copy()
-            eta = z @ r
-            thresh = (xf @ xf + 1e-16) * self.tol1 ** 2 + self.tol2 ** 2 * eta
-            for _ in range(self.cg_max):
-                if not eta >= thresh:
-                    break
-                w = self._Aff @ p
-                alf = eta / (p @ w)
-                y += alf * p
-                r -= alf * w
-                z = r * mdiag
-                eta_new = z @ r
-                p = z + (eta_new / eta) * p
-                eta = eta_new
-                self.solve_iterations += 1
-            x[self._free_idx] = xf + y
-            return torch.from_numpy(x)
+        """helm_solve: s + A+ res on the free edges (the device PCG)."""
         sv = self.solver
         sv.set("RES_E", res_e.detach().cpu().numpy())
         sv.set("S", s.detach().cpu().numpy())
@@ -364,10 +332,6 @@ class CavityModel:
 
     def matvec(self, x):
         """A x with the masked rows zeroed (the CG's operator)."""
-        if self.solver is None:
-            out = torch.zeros_like(x)
-            out[self._free_idx] = torch.from_numpy(self._Aff @ x.detach().cpu().numpy()[self._free_idx])
-            return out
         sv = self.solver
         sv.set("WORK_E", x.detach().cpu().numpy())
         sv.h.call("pyib_matvec", _lib.F["WORK_E"], _lib.F["WORK_E2"], C.c_double(self.dt), 1)

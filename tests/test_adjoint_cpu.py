@@ -10,7 +10,7 @@
 * the harmonic amplitude equals the restated fit of the reference's check tool;
 * the binomial checkpointing reverse sweep gives the gradient of the full tape
   while storing at most the allowed number of states;
-* in the checking mode (NumPy PCG of the device recurrence), the projected
+* with a NumPy mirror of the device PCG (``adjoint_cpu_model``), the projected
   pseudo-inverse of the singular cavity operator agrees with the solve on
   consistent vectors, and one whole step's adjoint (its solves see inconsistent
   gradients) matches central differences for the amplitude and the marker
@@ -23,6 +23,7 @@ import pytest
 import torch
 
 import parity_util as PU
+from adjoint_cpu_model import CpuCavityModel
 from pyib_b200 import adjoint as AD
 from pyib_b200 import harmonic as H
 from pyib_b200.cases import SphereCase
@@ -48,7 +49,7 @@ def cavity():
 @pytest.fixture(scope="module")
 def tiny():
     torch.set_num_threads(min(4, torch.get_num_threads()))
-    return AD.CavityModel(TINY, device="cpu", tol=1e-13)
+    return CpuCavityModel(TINY, tol=1e-13)
 
 
 def test_conv_diff_equals_reference(cavity):
