@@ -13,11 +13,12 @@ from pyib_b200.device import DeviceSolver
 pytestmark = pytest.mark.gpu
 
 
-def _solver(name="n3_osc"):
+def _solver(name="n3_osc", tol=None):
     g = PU.golden(name)
     lay = PU.layout_for(name)
+    kw = {} if tol is None else {"tol1": tol, "tol2": tol}
     sv = DeviceSolver(lay, rou=float(g["rou"]), visc=float(g["visc"]), cavity=bool(g["cavity"]),
-                      cg_max_iterations=5000)
+                      cg_max_iterations=20000, **kw)
     sv.set_markers(g["ib_markers"], g["ib_vel"], g["ib_ds"])
     return g, sv
 
@@ -32,10 +33,11 @@ def test_helmholtz_solve_adjoint_is_the_same_solve():
     """<c, A^-1 d> through autograd equals <A^-1 c, d> and the exact <A y, z>.
 
     d = A z and c = A y lie in the range of A (the closed cavity leaves a gauge
-    null space), so both solves have solutions; the CG stops at the reference's
-    relative tolerance, hence the 1e-6 bound.
+    null space), so both solves have solutions, and A being symmetric, <c, x> is
+    the same for every solution x.  The CG runs to a mixed tolerance of 1e-13, so
+    both sides agree with the exact value to 1e-9.
     """
-    g, sv = _solver()
+    g, sv = _solver(tol=1e-13)
     dt = float(g["dt"])
     free = sv.prec != 0.0
     rng = np.random.default_rng(5)
@@ -49,8 +51,10 @@ def test_helmholtz_solve_adjoint_is_the_same_solve():
     loss = (torch.tensor(c) * x).sum()
     loss.backward()
     adjoint = float(torch.dot(d_t.grad, torch.tensor(d)))
-    assert abs(loss.item() - exact) <= 1e-6 * abs(exact)
-    assert abs(adjoint - exact) <= 1e-6 * abs(exact)
+    print("solve adjoint: relative differences", abs(loss.item() - exact) / abs(exact),
+          abs(adjoint - exact) / abs(exact))
+    assert abs(loss.item() - exact) <= 1e-9 * abs(exact)
+    assert abs(adjoint - exact) <= 1e-9 * abs(exact)
     np.testing.assert_array_equal(s_t.grad.numpy(), c)       # d x / d s = identity
     assert np.all(d_t.grad.numpy()[~free] == 0.0)
 
@@ -89,7 +93,8 @@ def test_marker_position_gradient_matches_finite_differences():
     """d/dx of sum(w * interp(vc) at markers x) against a central difference.
 
     The Roma-Peskin kernel is continuously differentiable, so the difference
-    along a random direction converges to the kernel's Jacobian (step 1e-6 h).
+    along a random unit direction converges to the kernel's Jacobian (step 1e-6 h,
+    tolerance 1e-6 relative).
     """
     g, sv = _solver()
     rng = np.random.default_rng(9)
@@ -106,10 +111,12 @@ def test_marker_position_gradient_matches_finite_differences():
         return float((AG.MarkerInterpAt.apply(vc_t, torch.tensor(mk), sv, ds).numpy() * w).sum())
 
     direction = rng.standard_normal(mk0.shape)
+    direction /= np.linalg.norm(direction)
     eps = 1e-6 * sv.lay.h0
     fd = (f(mk0 + eps * direction) - f(mk0 - eps * direction)) / (2.0 * eps)
     ad = float(np.sum(ad_grad * direction))
-    assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+    print("interp position gradient: relative difference", abs(fd - ad) / abs(ad))
+    assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
     # per marker: the Jacobian of one marker's velocity along x
     m, c = 3, 0
     e = np.zeros_like(mk0)
@@ -118,7 +125,9 @@ def test_marker_position_gradient_matches_finite_differences():
     fm = AG.MarkerInterpAt.apply(vc_t, torch.tensor(mk0 - eps * e), sv, ds).numpy()[m, c]
     sv.set_markers(mk0, np.zeros_like(mk0), ds)
     jac = AG.interp_dx(sv, vc)
-    assert abs((fp - fm) / (2.0 * eps) - jac[m, c, 0]) <= 1e-5 * np.max(np.abs(jac[m])) + 1e-12
+    print("interp Jacobian entry: relative difference",
+          abs((fp - fm) / (2.0 * eps) - jac[m, c, 0]) / np.max(np.abs(jac[m])))
+    assert abs((fp - fm) / (2.0 * eps) - jac[m, c, 0]) <= 1e-6 * np.max(np.abs(jac[m])) + 1e-12
 
 
 
@@ -159,9 +168,11 @@ def test_marker_spread_position_gradient_matches_finite_differences():
         return float((AG.MarkerSpreadAt.apply(torch.tensor(ff), torch.tensor(mk), sv, ds).numpy() * h).sum())
 
     direction = rng.standard_normal(mk0.shape)
+    direction /= np.linalg.norm(direction)
     eps = 1e-6 * lay.h0
     fd = (loss(mk0 + eps * direction, f) - loss(mk0 - eps * direction, f)) / (2.0 * eps)
     ad = float(np.sum(ad_mk * direction))
-    assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+    print("spread position gradient: relative difference", abs(fd - ad) / abs(ad))
+    assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
     # linear in the forces: the gradient is exact
     assert abs(loss(mk0, f) - float(np.sum(ad_f * f))) <= 1e-12 * abs(loss(mk0, f))
