@@ -573,13 +573,15 @@ def run_adjoint(args):
     build.build_library()
     case = CASES["d16_adjoint_sphere" if args.workload == "d32_oscillating_sphere" else args.workload]
     steps = args.adjoint_steps
-    window = case.steps_per_period
+    window = args.adjoint_window or case.steps_per_period
     model = AD.CavityModel(case, tol=args.adjoint_tol)
     rng = np.random.default_rng(0)
     ref = model.ref0 + torch.from_numpy(0.01 * model.h0 * rng.standard_normal(tuple(model.ref0.shape))).to(model.dev)
     A, T = case.amplitude, case.period
     t0 = time.perf_counter()
-    J, gA, gT, gref, info = AD.force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20)
+    report = lambda text: print("#", text, file=sys.stderr, flush=True)
+    J, gA, gT, gref, info = AD.force_amplitude_and_gradient(model, A, T, ref, steps, window,
+                                                            snapshots=args.adjoint_snapshots, progress=report)
     t_grad = time.perf_counter() - t0
     print("# gradient", json.dumps({"J": J, "dJ_dA": gA, "dJ_dT": gT, "seconds": t_grad}), file=sys.stderr, flush=True)
     fd = {}
@@ -608,7 +610,9 @@ def run_adjoint(args):
             "relative_differences": rel, "max_stored_states": info["max_stored_states"],
             "recomputed_steps": info["recomputed_steps"], "forward_cg_iterations": info["forward_cg_iterations"],
             "total_cg_iterations": info["total_cg_iterations"], "cell_cg_iterations": info["cell_cg_iterations"],
-            "gradient_seconds": t_grad, "finite_difference_seconds": t_fd, "tolerance": args.adjoint_tol}
+            "gradient_seconds": t_grad, "finite_difference_seconds": t_fd, "tolerance": args.adjoint_tol,
+            "snapshots": args.adjoint_snapshots,
+            "seconds": {k: info[k] for k in ("forward_seconds", "solve_seconds", "cell_solve_seconds")}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -1005,6 +1009,9 @@ def main():
     ap.add_argument("--adjoint-fd", default="A,T,dir0",
                     help="comma list of central-difference checks: A, T, dir0, dir1, ...")
     ap.add_argument("--adjoint-tol", type=float, default=1e-13)
+    ap.add_argument("--adjoint-window", type=int, default=0,
+                    help="steps fitted at the end (default: one period of the configuration)")
+    ap.add_argument("--adjoint-snapshots", type=int, default=20)
     ap.add_argument("--matvec-only", action="store_true",
                     help="time the standalone float64 matvecs (three-kernel and fused) on the workload's layout")
     ap.add_argument("--compare-precision", action="store_true",

@@ -41,6 +41,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import time
 
 import numpy as np
 import scipy.sparse as sp
@@ -270,6 +271,12 @@ class CavityModel:
         ops, prec = self._setup_solver(device)
         d = self.dev
         step_operators(lay, ops, self.visc, d, into=self)
+        # Jacobi preconditioner of K = T M T^T (cells): diag K = (T o T) diag M
+        Tm = (sp.hstack([ops.I[0], ops.I[1], ops.I[2]]).T @ ops.C).tocsr()
+        dK = Tm.multiply(Tm) @ np.asarray(prec, dtype=np.float64)
+        self.kdiag_inv = torch.from_numpy(np.where(dK > 0.0, 1.0 / np.where(dK > 0.0, dK, 1.0), 0.0)).to(d)
+        self._k_prev = None
+        self.seconds = {"solve": 0.0, "cells": 0.0}
         self.free = torch.from_numpy((prec != 0.0).astype(np.float64)).to(d)
         self.prec_t = torch.from_numpy(np.asarray(prec, dtype=np.float64)).to(d)
         # immersed boundary: finest-level lattice (ib_immersed.py:29-40)
@@ -322,6 +329,13 @@ class CavityModel:
 
     def solve(self, res_e, s):
         """helm_solve: s + A+ res on the free edges (the device PCG)."""
+        t0 = time.perf_counter()
+        try:
+            return self._solve_device(res_e, s)
+        finally:
+            self.seconds["solve"] += time.perf_counter() - t0
+
+    def _solve_device(self, res_e, s):
         sv = self.solver
         sv.set("RES_E", res_e.detach().cpu().numpy())
         sv.set("S", s.detach().cpu().numpy())
@@ -345,23 +359,27 @@ class CavityModel:
         """T^T k = rot integr_c2f k: the residual map of the step."""
         return self.Rop.M @ (self.Iop.M @ k)
 
-    def _cg(self, op, b, tol, check=10):
-        """Plain CG from zero for a consistent symmetric positive semi-definite system."""
-        x = torch.zeros_like(b)
-        r = b.clone()
-        p = r.clone()
-        rr = r @ r
-        stop = (tol * tol) * rr
+    def _cg(self, op, b, tol, x0=None, dinv=None, check=10):
+        """CG for a consistent symmetric positive semi-definite system, from ``x0``
+        (zero if None), preconditioned by the diagonal ``dinv`` (none if None);
+        stops when |r| <= tol |b| (tested every ``check`` iterations)."""
+        x = torch.zeros_like(b) if x0 is None else x0.clone()
+        r = b.clone() if x0 is None else b - op(x)
+        stop = (tol * tol) * (b @ b)
+        z = r if dinv is None else dinv * r
+        p = z.clone()
+        rz = r @ z
         for it in range(self.cg_max):
-            if it % check == 0 and not bool(rr > stop):
+            if it % check == 0 and not bool((r @ r) > stop):
                 break
             Ap = op(p)
-            a = rr / (p @ Ap)
+            a = rz / (p @ Ap)
             x += a * p
             r -= a * Ap
-            rr_new = r @ r
-            p = r + (rr_new / rr) * p
-            rr = rr_new
+            z = r if dinv is None else dinv * r
+            rz_new = r @ z
+            p = z + (rz_new / rz) * p
+            rz = rz_new
             self.cell_iterations += 1
         return x
 
@@ -372,11 +390,17 @@ class CavityModel:
         volumes), so the null space of A is the null space of T, and downstream the
         solve's gradient is only used through T.  A+ acts on the projection of
         M^1/2 g onto the range of M^1/2 T^T, which is M^1/2 T^T K+ T M g with
-        K = T M T^T: one CG solve with K on cell vectors, after which A+ (T^T k)
-        is a consistent solve by the device PCG.
+        K = T M T^T: one CG solve with K on cell vectors (Jacobi-preconditioned,
+        started from the previous call's k, which the reverse sweep's consecutive
+        solves keep close), after which A+ (T^T k) is a consistent solve by the
+        device PCG.
         """
-        k = self._cg(lambda v: self._T(self.prec_t * self._Tt(v)), self._T(self.prec_t * g), self.tol2)
+        t0 = time.perf_counter()
+        k = self._cg(lambda v: self._T(self.prec_t * self._Tt(v)), self._T(self.prec_t * g), self.tol2,
+                     x0=self._k_prev, dinv=self.kdiag_inv)
+        self._k_prev = k
         u = self._Tt(k) * self.free
+        self.seconds["cells"] += time.perf_counter() - t0
         return self.solve(u, torch.zeros_like(g)) * self.free
 
     # ---- the step's pieces ------------------------------------------------------------
@@ -487,6 +511,9 @@ class Reverser:
         self.recomputed = 0
         self.max_live = 1                  # the initial state is stored throughout
         self._live = 0
+        self.progress = None
+        self._reversed = 0
+        self._t0 = time.perf_counter()
 
     def advance(self, state, i0, i1):
         with torch.no_grad():
@@ -506,6 +533,11 @@ class Reverser:
             grads = torch.autograd.grad(outs, inp + params, grad_outputs=gouts, allow_unused=True)
         k = len(inp)
         self.lam = [g if g is not None else torch.zeros_like(x) for g, x in zip(grads[:k], inp)]
+        self._reversed += 1
+        if self.progress is not None and self._reversed % 20 == 0:
+            self.progress(f"reversed {self._reversed} steps (at step {n}), {self.recomputed} recomputed, "
+                          f"{time.perf_counter() - self._t0:.1f} s, {self.m.solve_iterations} PCG and "
+                          f"{self.m.cell_iterations} cell CG iterations")
         for j, g in enumerate(grads[k:]):
             if g is not None:
                 self.grad[j] = self.grad[j] + g.detach()
@@ -558,17 +590,24 @@ def force_amplitude(model, A, T, ref, steps, window):
     return float(harmonic_amplitude(F[steps - window:], times[steps - window:], om_t, model.phase))
 
 
-def force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20):
+def force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20, progress=None):
     """J = harmonic amplitude of the axial body force over the last ``window`` steps,
     and dJ/dA, dJ/dT, dJ/dref by the discrete adjoint with binomial checkpointing.
 
     ``A`` and ``T`` are floats, ``ref`` the (M, 3) reference marker positions.
-    Returns (J, dJ/dA, dJ/dT, dJ/dref (M, 3), info).
+    ``progress`` (optional) is called with a short text after the forward run and
+    every 20 reverse steps.  Returns (J, dJ/dA, dJ/dT, dJ/dref (M, 3), info).
     """
     A_t, om_t, ref_t = _params(model, A, T, ref)
     model.solve_iterations = model.cell_iterations = 0
+    model.seconds = {"solve": 0.0, "cells": 0.0}
+    model._k_prev = None
+    t0 = time.perf_counter()
     state0, state, F = _history(model, A_t, om_t, ref_t, steps)
     fwd_iters = model.solve_iterations
+    t_fwd = time.perf_counter() - t0
+    if progress is not None:
+        progress(f"forward {steps} steps {t_fwd:.1f} s, {fwd_iters} CG iterations")
     times = torch.arange(1, steps + 1, dtype=torch.float64, device=model.dev) * model.dt
     Fw = F.detach().clone().requires_grad_(True)
     om_f = om_t.detach().clone().requires_grad_(True)
@@ -577,6 +616,7 @@ def force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20):
         gF, g_om_fit = torch.autograd.grad(J, [Fw, om_f])
     # reverse sweep; J depends on the forces, so the final state's adjoint is zero
     rv = Reverser(model, (A_t, om_t, ref_t), gF, snapshots)
+    rv.progress = progress
     rv.lam = [torch.zeros_like(x) for x in state]
     rv.reverse(state0, 0, steps, snapshots - 1)
     # the initial state depends on the parameters only through its interior momentum
@@ -593,6 +633,8 @@ def force_amplitude_and_gradient(model, A, T, ref, steps, window, snapshots=20):
     dJdT = gom * (-2.0 * math.pi / float(T) ** 2)
     info = {"forward_cg_iterations": fwd_iters, "total_cg_iterations": model.solve_iterations,
             "cell_cg_iterations": model.cell_iterations, "recomputed_steps": rv.recomputed,
+            "forward_seconds": t_fwd, "solve_seconds": model.seconds["solve"],
+            "cell_solve_seconds": model.seconds["cells"],
             "max_stored_states": rv.max_live, "force": F.cpu().numpy()}
     return float(J), float(gA), float(dJdT), gref.cpu().numpy(), info
 
