@@ -362,10 +362,18 @@ class CavityModel:
     def _cg(self, op, b, tol, x0=None, dinv=None, check=10):
         """CG for a consistent symmetric positive semi-definite system, from ``x0``
         (zero if None), preconditioned by the diagonal ``dinv`` (none if None);
-        stops when |r| <= tol |b| (tested every ``check`` iterations)."""
-        x = torch.zeros_like(b) if x0 is None else x0.clone()
-        r = b.clone() if x0 is None else b - op(x)
-        stop = (tol * tol) * (b @ b)
+        stops when |r| <= tol |b| (tested every ``check`` iterations).  A start that
+        does not reduce the residual below |b| is replaced by zero, and b = 0
+        returns zero."""
+        bb = b @ b
+        if not bool(bb > 0.0):
+            return torch.zeros_like(b)
+        stop = (tol * tol) * bb
+        x, r = torch.zeros_like(b), b.clone()
+        if x0 is not None:
+            r0 = b - op(x0)
+            if bool((r0 @ r0) < bb):
+                x, r = x0.clone(), r0
         z = r if dinv is None else dinv * r
         p = z.clone()
         rz = r @ z
@@ -373,7 +381,10 @@ class CavityModel:
             if it % check == 0 and not bool((r @ r) > stop):
                 break
             Ap = op(p)
-            a = rz / (p @ Ap)
+            pAp = p @ Ap
+            if it % check == 0 and not bool(pAp > 0.0):
+                break                      # the residual left is in the null space
+            a = rz / pAp
             x += a * p
             r -= a * Ap
             z = r if dinv is None else dinv * r

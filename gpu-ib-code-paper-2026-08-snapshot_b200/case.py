@@ -151,7 +151,12 @@ def validate_config(raw: dict) -> dict:
         raise CaseConfigError("runtime.device must be 'b200' here ('cpu'/'cuda' are the reference's backends)")
     if rt["precision"] not in {"float64", "mixed"}:
         raise CaseConfigError("runtime.precision must be 'float64' or 'mixed'")
-    rt["mixed_tolerance"] = _positive("runtime.mixed_tolerance", rt.get("mixed_tolerance", 0.1))
+    # the mixed form's update tolerance; absent from a float64 configuration, whose
+    # runtime block keeps the reference's keys
+    if rt["precision"] == "mixed":
+        rt["mixed_tolerance"] = _positive("runtime.mixed_tolerance", rt.get("mixed_tolerance", 0.1))
+    else:
+        rt.pop("mixed_tolerance", None)
     mesh = cfg["mesh"]
     mk = str(mesh["kind"])
     if mk not in {"uniform_box", "sphere_concentric", "sphere_wake", "nested_boxes"}:
@@ -305,7 +310,7 @@ def build_runtime(cfg) -> CaseRuntime:
     so = cfg["solver"]
     drv = B200Driver(lay, visc=rho * nu, rou=rho, cg_max_iterations=so["cg_max_iterations"],
                      fail_on_cg_nonconvergence=so["fail_on_cg_nonconvergence"],
-                     precision=cfg["runtime"]["precision"], mixed_tol=cfg["runtime"]["mixed_tolerance"])
+                     precision=cfg["runtime"]["precision"], mixed_tol=cfg["runtime"].get("mixed_tolerance", 0.1))
     drv.cg_check_interval = so["cg_check_interval"]
     if cfg["mesh"]["kind"] in {"sphere_concentric", "nested_boxes"}:
         drv.set_cavity(U_lid=0.0, spanwise_zerograd=False)
@@ -455,16 +460,24 @@ def mesh_summary(rt: CaseRuntime) -> dict:
     cfg, lay = rt.config, rt.layout
     desc, _ = rt.driver.reference_maps()
     mesh = cfg["mesh"]
-    out = {"kind": mesh["kind"], "cells": int(lay.cell_active.sum()), "faces": int(lay.face_exists.sum()),
-           "edges": int(lay.edge_exists.sum()), "nodes": int(desc["nodes"].shape[0]),
+    out = {"kind": mesh["kind"], "faces": int(lay.face_exists.sum()), "edges": int(lay.edge_exists.sum()),
            "markers": int(rt.reference_markers.shape[0])}
     if mesh["kind"] == "uniform_box":
-        out.update(dx=float(mesh["dx"]), bounds=[list(map(float, b)) for b in mesh["bounds"]])
+        out.update(cells=int(lay.cell_active.sum()), dx=float(mesh["dx"]),
+                   bounds=[list(map(float, b)) for b in mesh["bounds"]])
     else:
         D = 2.0 * float(cfg["ib"]["radius"])
         per = [int(np.count_nonzero(lay.cell_active & (lay.cell_level == L))) for L in range(lay.N)]
+        # the analytic counts: each level's box minus the box of the finer level inside it
+        expected = [int(np.prod(lv.n)) - (int(np.prod(lay.levels[L - 1].n)) // 8 if L > 0 else 0)
+                    for L, lv in enumerate(lay.levels)]
+        top = lay.levels[-1]
         out.update(D_over_dx=int(mesh["cells_per_diameter"]), diameter=D, dx_fine=float(rt.dx),
-                   layer_cells=per, total_cells=int(sum(per)),
+                   outer_domain_D={ax: [float(top.lo[a] / D), float((top.lo[a] + top.n[a] * top.h) / D)]
+                                   for a, ax in enumerate("xyz")},
+                   layer_cells=per, expected_layer_cells=expected,
+                   total_cells=int(sum(per)), expected_total_cells=int(sum(expected)),
+                   nodes=int(desc["nodes"].shape[0]),
                    layer_spacing_D=[float(lv.h / D) for lv in lay.levels],
                    layer_bounds_D=[[float((lv.lo[a] + s * lv.n[a] * lv.h) / D)
                                     for a in range(3) for s in (0, 1)] for lv in lay.levels])

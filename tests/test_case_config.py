@@ -21,7 +21,10 @@ def test_defaults_and_normalisation():
     cfg = CS.validate_config(SMOKE)
     assert cfg["solver"]["cg_check_interval"] == 20
     assert cfg["ib"]["motion"]["axis"] == [0.0, 1.0, 0.0]
-    assert cfg["runtime"]["mixed_tolerance"] == pytest.approx(0.1)
+    assert "mixed_tolerance" not in cfg["runtime"]          # float64: the reference's runtime keys
+    mixed = json.loads(json.dumps(SMOKE))
+    mixed["runtime"]["precision"] = "mixed"
+    assert CS.validate_config(mixed)["runtime"]["mixed_tolerance"] == pytest.approx(0.1)
 
 
 @pytest.mark.parametrize("patch, msg", [
