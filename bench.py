@@ -55,6 +55,30 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def matvec_plan(sv):
+    """The autotuner's matvec plan: per precision, whether it ran, the cell- and
+    node-tile z depths, and whether curl+interp and viscous run as one kernel."""
+    out = (C.c_int32 * 8)()
+    sv.h.call("pyib_matvec_plan", out)
+    plan = {}
+    for q, name in enumerate(("float64", "float32")):
+        t, kz, kzr, av = (int(x) for x in out[4 * q:4 * q + 4])
+        if t:
+            plan[name] = {"cell_tile": [32, 8, kz], "node_tile": [32, 8, kzr], "curl_interp_viscous_fused": bool(av)}
+    return plan
+
+
+def matvec_kernel_ms(mv, fused_av):
+    """Per-kernel times of pyib_bench_matvec (slots 1..6) under the kernels' names."""
+    if fused_av:
+        names = ["curl_interp_viscous", "curl_interp_patch", None, "viscous_patch", "integr_rot_dot",
+                 "integr_rot_patch_reduce"]
+    else:
+        names = ["curl_interp", "curl_interp_patch", "viscous", "viscous_patch", "integr_rot_dot",
+                 "integr_rot_patch_reduce"]
+    return {n: float(x) for n, x in zip(names, list(mv)[1:7]) if n is not None}
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
 
@@ -412,7 +436,8 @@ def run_b200(args, world, rank, local):
     sv.h.call("pyib_event", 1, C.byref(ev_ms))
     sv.h.call("pyib_cg_timing", timing, 1)
     cg_s, cg_it, launches = float(timing[0]), float(timing[1]), int(timing[2])
-    tiles = {"cell_tile": [32, 8, int(timing[3])], "node_tile": [32, 8, int(timing[4])]}
+    tiles = matvec_plan(sv).get("float64", {})
+    av = bool(tiles.get("curl_interp_viscous_fused", False))
     t_dev = ev_ms.value / 1000.0
     barrier(dist)
     # e2e: the same steps again from the same state, through the public API, with the
@@ -440,8 +465,7 @@ def run_b200(args, world, rank, local):
     sv.set("WORK_E", np.random.default_rng(0).standard_normal(sv.lay.NE) * sv.lay.edge_exists)
     sv.h.call("pyib_bench_matvec", 50, C.c_double(run.dt), mv)
     mv_ms = C.c_double(mv[0])
-    mv_kernels = dict(zip(["curl_interp", "curl_interp_patch", "viscous", "viscous_patch", "integr_rot_dot",
-                           "integr_rot_patch_reduce"], [float(x) for x in mv[1:7]]))
+    mv_kernels = matvec_kernel_ms(mv, av)
     mvf = (C.c_double * 6)()
     sv.h.call("pyib_bench_matvec_fused", 50, C.c_double(run.dt), mvf)
     mvf_kernels = dict(zip(["exact_vc_rows_and_list", "exact_vq_rows", "k_mvF", "exact_w_rows_dot"],
@@ -493,15 +517,17 @@ def run_b200(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": ("PCG iteration (fused matvec k_mvF with its exact rows + update + direction)"
-                                    if fused else "PCG iteration (matvec A/V/RI + update + direction)"),
+                                    if fused else
+                                    "PCG iteration (matvec AV/RI + update + direction)" if av else
+                                    "PCG iteration (matvec A/V/RI + update + direction)"),
                          "algorithmic_bytes_per_launch": ALGO_BYTES_PER_EDGE_ITER * ne,
                          "peak_kind": peak_kind},
             "matvec": {"fused": {"ms": float(mvf[0]), "achieved_gbs": mvf_achieved, "frac": mvf_achieved / peak,
                                  "kernel_ms": mvf_kernels, "node_planes_per_block": int(mvf[5])},
-                       "three_kernel": {"ms": mv_ms.value, "achieved_gbs": mv_achieved,
-                                        "frac": mv_achieved / peak, "kernel_ms": mv_kernels},
+                       "tuned": {"ms": mv_ms.value, "achieved_gbs": mv_achieved, "frac": mv_achieved / peak,
+                                 "form": "AV, RI" if av else "A, V, RI", "kernel_ms": mv_kernels},
                        "algorithmic_bytes": ALGO_BYTES_PER_EDGE_MATVEC * ne,
-                       "used_by_cg": "fused" if fused else "three_kernel"},
+                       "used_by_cg": "fused" if fused else "tuned"},
             "cg": {"seconds": cg_s, "iterations": cg_it, "ms_per_iteration": 1e3 * t_iter,
                    "gbs": achieved},
             "gpu_launches": launches,
@@ -522,9 +548,11 @@ def run_b200(args, world, rank, local):
 def run_matvec(args):
     """Standalone float64 matvec timings on a workload's layout (no time stepping).
 
-    Prints one JSON line with the three-kernel matvec (``pyib_bench_matvec``) and
-    the single-pass fused matvec (``pyib_bench_matvec_fused``), each averaged over
-    50 calls with CUDA events, and their algorithmic HBM rates (16 B per edge).
+    Prints one JSON line with the autotuned matvec (``pyib_bench_matvec``: curl+interp
+    and viscous apart or fused, then integr+rot, whichever the tuner picked; pin one
+    with PYIB_MATVEC_AV=0/1) and the single-pass fused matvec
+    (``pyib_bench_matvec_fused``), each averaged over 50 calls with CUDA events, and
+    their algorithmic HBM rates (16 B per edge).
     """
     import _pyib_b200_import
     _pyib_b200_import.load()
@@ -538,15 +566,15 @@ def run_matvec(args):
     sv.set("WORK_E", np.random.default_rng(0).standard_normal(lay.NE) * lay.edge_exists)
     three = (C.c_double * 7)()
     sv.h.call("pyib_bench_matvec", 50, C.c_double(case.time_step), three)
+    av = bool(matvec_plan(sv).get("float64", {}).get("curl_interp_viscous_fused", False))
     fused = (C.c_double * 6)()
     sv.h.call("pyib_bench_matvec_fused", 50, C.c_double(case.time_step), fused)
     ne = int(lay.edge_exists.sum())
     peak, peak_kind = peaks()
     gbs = lambda ms: ALGO_BYTES_PER_EDGE_MATVEC * ne / (ms / 1e3) / 1e9
     line = {"workload": case.name, "edges": ne, "cells": int(lay.cell_active.sum()),
-            "three_kernel": {"ms": three[0], "gbs": gbs(three[0]), "kernel_ms": dict(zip(
-                ["curl_interp", "curl_interp_patch", "viscous", "viscous_patch", "integr_rot_dot",
-                 "integr_rot_patch_reduce"], list(three)[1:]))},
+            "tuned": {"ms": three[0], "gbs": gbs(three[0]), "form": "AV, RI" if av else "A, V, RI",
+                      "kernel_ms": matvec_kernel_ms(three, av)},
             "fused": {"ms": fused[0], "gbs": gbs(fused[0]), "kz": int(fused[5]), "kernel_ms": dict(zip(
                 ["exact_vc_rows_and_list", "exact_vq_rows", "k_mvF", "exact_w_rows_dot"], list(fused)[1:5]))},
             "peak_gbs": peak, "peak_kind": peak_kind}
@@ -642,14 +670,14 @@ def mixed_leg(case, tables, args, steps_done, final):
     mv = (C.c_double * 7)()
     sv.set("WORK_E", np.random.default_rng(0).standard_normal(sv.lay.NE) * sv.lay.edge_exists)
     sv.h.call("pyib_bench_matvec", 50, C.c_double(run.dt), mv)
-    kernels = dict(zip(["matvec", "curl_interp", "curl_interp_patch", "viscous", "viscous_patch",
-                        "integr_rot_dot", "integr_rot_patch_reduce"], [float(x) for x in mv]))
+    plan32 = matvec_plan(sv).get("float32", {})
+    kernels = {"matvec": float(mv[0]), **matvec_kernel_ms(mv, plan32.get("curl_interp_viscous_fused", False))}
     sv.h.close()
     t = ev.value / 1000.0
     return {"value": args.steps / t, "unit": "steps/s", "ms_per_step": 1000.0 * t / args.steps,
             "inner_iterations_per_step": its / args.steps, "mixed_tolerance": args.mixed_tol,
             "errors_vs_float64_after_steps": steps_done, "errors_vs_float64": err,
-            "float32_matvec_kernel_ms": kernels}
+            "float32_matvec_kernel_ms": kernels, "float32_matvec_plan": plan32}
 
 
 # ---------------------------------------------------------------------------

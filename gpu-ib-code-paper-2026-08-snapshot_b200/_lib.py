@@ -41,7 +41,7 @@ EXPORTS = [
     "pyib_set_params", "pyib_set_ib_geometry", "pyib_set_field", "pyib_get_field", "pyib_matvec",
     "pyib_operator", "pyib_calc_vel", "pyib_conv_diff", "pyib_helm_solve", "pyib_step",
     "pyib_ib_stencil", "pyib_ib_interp", "pyib_ib_spread", "pyib_loads", "pyib_diagnostics",
-    "pyib_cg_timing", "pyib_event", "pyib_bench_matvec", "pyib_bench_matvec_fused", "pyib_spread_noalloc", "pyib_ib_interp_dx", "pyib_graph_pcg",
+    "pyib_cg_timing", "pyib_matvec_plan", "pyib_event", "pyib_bench_matvec", "pyib_bench_matvec_fused", "pyib_spread_noalloc", "pyib_ib_interp_dx", "pyib_graph_pcg",
     "pyib_recover_pressure",
 ]
 
@@ -133,6 +133,7 @@ def load():
                        C.POINTER(C.c_double), C.POINTER(C.c_double)],
         "pyib_diagnostics": [vp, C.POINTER(C.c_double)],
         "pyib_cg_timing": [vp, C.POINTER(C.c_double), C.c_int32],
+        "pyib_matvec_plan": [vp, C.POINTER(C.c_int32)],
         "pyib_event": [vp, C.c_int32, C.POINTER(C.c_double)],
         "pyib_bench_matvec": [vp, C.c_int32, C.c_double, C.POINTER(C.c_double)],
         "pyib_bench_matvec_fused": [vp, C.c_int32, C.c_double, C.POINTER(C.c_double)],

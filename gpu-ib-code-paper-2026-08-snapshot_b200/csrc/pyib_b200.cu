@@ -70,6 +70,7 @@ struct Meta {
   int nplanes;         // per-plane partial sums of kernel RI (independent of the z-chunk depth)
   int ri_up;           // 1: kernel RI also marches the upper-face nodes (i = nx, j = ny, k = nz);
                        // 0: every upper-face edge is an exact (patch) row or masked
+  int av;              // 1: kernels A and V run fused (k_mvAV); 0: as two kernels
   int kzF;             // node planes marched by one block of the fused matvec
   int gxF, gyF, gzF;   // fused-matvec grid
   int nplanesF;        // per-plane partial sums of the fused matvec
@@ -151,7 +152,9 @@ struct pyib_ctx {
   int cg_graph_alpd = -1;
   // fused single-pass matvec of the float64 CG (k_mvF)
   bool use_fused = false;        // PYIB_FUSED_MATVEC=1 selects the single-pass matvec in the CG
+  int av_pin = -1;               // PYIB_MATVEC_AV: -1 tuned, 0 kernels A and V apart, 1 fused
   bool fused_ready = false;
+  bool flags_ready = false;      // f_* cell flags and the f_list of the fused kernels
   bool tunedF = false;
   unsigned int *f_irrA = nullptr, *f_irrV = nullptr, *f_needR = nullptr;
   unsigned char* f_flags = nullptr;   // per cell: exact vc / exact vq / store vq
@@ -486,6 +489,207 @@ __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v
     }
     src += cs;
     dst += cs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// matvec kernel AV: vq = V P C p in one pass (kernels A and V fused), so the cell
+// intermediate vc stays on chip.  Thread (tx,ty) of a 32x8 cell tile marches KZ cell
+// planes in z and computes vc one plane ahead of the viscous row that needs it.  The
+// x/y neighbours of the 7-point template come from a two-plane shared-memory buffer
+// holding vc of the tile and of its one-cell ring; the z neighbours stay in registers.
+// The ring columns are marched by warps 0-2 (warp 0 the row below the tile, warp 1 the
+// row above, warp 2 the columns left (lanes 0-7) and right (lanes 16-23)); every
+// column carries its upper x- and y-edge values to the next plane, as kernel A does.
+// Cells with exact vc rows (kFlagExactVc) take vc from vcm, where k_patchA wrote it
+// before this kernel; the template vc of the cells an exact V row reads (kFlagStoreVc)
+// is stored to vcm for k_patchV, which runs after this kernel and overwrites the vq
+// of irregular cells.  Every row is the expression of k_mvA and k_mvV term for term,
+// so vq is bit-identical to the two-kernel path.
+// ---------------------------------------------------------------------------
+// per-cell flags of the fused matvec kernels: exact vc row (k_patchA), exact vq row
+// (k_patchV), vq read by an exact w row (k_mvF stores it), template vc read by an
+// exact vq row (k_mvAV stores it)
+constexpr unsigned char kFlagExactVc = 1, kFlagExactVq = 2, kFlagStoreVq = 4, kFlagStoreVc = 8;
+
+template <typename T>
+struct AVCol {
+  int ox, oy, oz;          // x-, y-, z-edge offsets of the column's cell on the next plane
+  T ex0, ex1, ey0, ey1;    // x-edges (i,j), (i,j+1) and y-edges (i,j), (i+1,j) of that plane
+};
+
+template <typename T>
+__device__ __forceinline__ void av_col_start(AVCol<T>& c, const T* ex, const T* ey, int nx, int ny, int i, int j,
+                                             int k) {
+  c.ox = (k * (ny + 1) + j) * nx + i;
+  c.oy = (k * ny + j) * (nx + 1) + i;
+  c.oz = (k * (ny + 1) + j) * (nx + 1) + i;
+  c.ex0 = ex[c.ox];
+  c.ex1 = ex[c.ox + nx];
+  c.ey0 = ey[c.oy];
+  c.ey1 = ey[c.oy + 1];
+}
+
+// template vc of the column's cell on its next plane when tmpl (else v is left as is),
+// then the column moves up one plane
+template <typename T>
+__device__ __forceinline__ void av_col_step(AVCol<T>& c, const T* ex, const T* ey, const T* ez, int nx, int sxk,
+                                            int syk, int szk, T s, bool tmpl, T (&v)[3]) {
+  const T ex01 = ex[c.ox + sxk], ex11 = ex[c.ox + sxk + nx];
+  const T ey01 = ey[c.oy + syk], ey11 = ey[c.oy + syk + 1];
+  // the z-edges are loaded whatever the cell's flag (they exist for every cell of the
+  // level's box), so these loads are not held up by the flag load
+  const T ez00 = ez[c.oz], ez10 = ez[c.oz + 1], ez01 = ez[c.oz + nx + 1], ez11 = ez[c.oz + nx + 2];
+  if (tmpl) {
+    const T ux0 = c.ey0 + ez01 - ey01 - ez00;
+    const T ux1 = c.ey1 + ez11 - ey11 - ez10;
+    const T uy0 = ez00 + ex01 - ez10 - c.ex0;
+    const T uy1 = ez01 + ex11 - ez11 - c.ex1;
+    const T uz0 = c.ex0 + c.ey1 - c.ex1 - c.ey0;
+    const T uz1 = ex01 + ey11 - ex11 - ey01;
+    v[0] = (ux0 + ux1) * s;
+    v[1] = (uy0 + uy1) * s;
+    v[2] = (uz0 + uz1) * s;
+  }
+  c.ex0 = ex01;
+  c.ex1 = ex11;
+  c.ey0 = ey01;
+  c.ey1 = ey11;
+  c.ox += sxk;
+  c.oy += syk;
+  c.oz += szk;
+}
+
+// vc of cell (i,j,k) of the column: exact (vcm), zero in the hole, else the template
+template <typename T>
+__device__ __forceinline__ void av_col_vc(AVCol<T>& c, const LevelMeta& l, const T* ex, const T* ey, const T* ez,
+                                          const T* vcm, const unsigned char* __restrict__ flags, long long nc,
+                                          int sxk, int syk, int szk, T s, bool col_hole, int i, int j, int k,
+                                          unsigned char& f, T (&v)[3]) {
+  const int nx = l.n[0], ny = l.n[1];
+  const long long cell = l.cbase + ((long long)k * ny + j) * nx + i;
+  f = flags[cell];
+  const bool hole = col_hole && k >= l.hole_lo[2] && k < l.hole_hi[2];
+  const bool exact = (f & kFlagExactVc) != 0;
+  av_col_step<T>(c, ex, ey, ez, nx, sxk, syk, szk, s, !hole && !exact, v);
+  if (exact) {
+    v[0] = vcm[cell];
+    v[1] = vcm[nc + cell];
+    v[2] = vcm[2 * nc + cell];
+  } else if (hole) {
+    v[0] = v[1] = v[2] = (T)0;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY, sizeof(T) == 8 ? 3 : 4) k_mvAV(Meta m, const T* __restrict__ p, T* vcm, T* __restrict__ vq,
+                                                   const unsigned char* __restrict__ flags,
+                                                   const CGState* __restrict__ st) {
+  static_assert(TX == 32 && TY == 8, "the ring assignment below assumes 32 x 8 tiles");
+  if (st->done) return;
+  __shared__ T sv[2][3][TY + 2][TX + 2];
+  const int L = level_of_zblock(m, blockIdx.z, false);
+  const LevelMeta& l = m.lv[L];
+  const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  if (i0 >= nx || j0 >= ny) return;   // the whole block lies outside this level
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = i < nx && j < ny;
+  const int k0 = (blockIdx.z - l.zbA) * m.kz;
+  const int k1 = min(k0 + m.kz, nz);
+  const long long nc = m.nc;
+  const T* ex = p + l.ebase[0];
+  const T* ey = p + l.ebase[1];
+  const T* ez = p + l.ebase[2];
+  const int sxk = (ny + 1) * nx, syk = ny * (nx + 1), szk = (ny + 1) * (nx + 1);
+  const T s = (T)(1.0 / (2.0 * l.h * l.h));
+  const T rou = (T)st->rou, kf = (T)st->kfac;
+  const T inv_h2 = (T)(1.0 / (l.h * l.h));
+  auto in_hole_col = [&](int a, int b) {
+    return l.has_hole && a >= l.hole_lo[0] && a < l.hole_hi[0] && b >= l.hole_lo[1] && b < l.hole_hi[1];
+  };
+  // ring column of this thread (shared-memory slot sx, sy), if any
+  int hi = -1, hj = -1, sx = 0, sy = 0;
+  if (ty == 0) { hi = i; hj = j0 - 1; sx = tx + 1; sy = 0; }
+  else if (ty == 1) { hi = i; hj = j0 + TY; sx = tx + 1; sy = TY + 1; }
+  else if (ty == 2 && tx < TY) { hi = i0 - 1; hj = j0 + tx; sx = 0; sy = tx + 1; }
+  else if (ty == 2 && tx >= 16 && tx < 16 + TY) { hi = i0 + TX; hj = j0 + tx - 16; sx = TX + 1; sy = tx - 15; }
+  const bool ring = hi >= 0 && hi < nx && hj >= 0 && hj < ny;
+  const bool own_hole = in_hole_col(i, j), ring_hole = ring && in_hole_col(hi, hj);
+  const int kstart = k0 > 0 ? k0 - 1 : 0;
+  AVCol<T> oc, rc;
+  if (own) av_col_start<T>(oc, ex, ey, nx, ny, i, j, kstart);
+  if (ring) av_col_start<T>(rc, ex, ey, nx, ny, hi, hj, kstart);
+  T vm[3] = {0, 0, 0}, v0[3] = {0, 0, 0}, vp[3] = {0, 0, 0}, hv[3] = {0, 0, 0};
+  unsigned char f = 0;
+  if (k0 > 0) {
+    // plane k0-1: the own column's z-lower neighbour; the ring column only moves up
+    if (own) av_col_vc<T>(oc, l, ex, ey, ez, vcm, flags, nc, sxk, syk, szk, s, own_hole, i, j, k0 - 1, f, vm);
+    if (ring) av_col_step<T>(rc, ex, ey, ez, nx, sxk, syk, szk, s, false, hv);
+  }
+  if (own) {
+    av_col_vc<T>(oc, l, ex, ey, ez, vcm, flags, nc, sxk, syk, szk, s, own_hole, i, j, k0, f, v0);
+    if (f & kFlagStoreVc) {
+      const long long cell = l.cbase + ((long long)k0 * ny + j) * nx + i;
+      vcm[cell] = v0[0];
+      vcm[nc + cell] = v0[1];
+      vcm[2 * nc + cell] = v0[2];
+    }
+  }
+  if (ring) av_col_vc<T>(rc, l, ex, ey, ez, vcm, flags, nc, sxk, syk, szk, s, ring_hole, hi, hj, k0, f, hv);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    sv[0][d][ty + 1][tx + 1] = v0[d];
+    if (ring) sv[0][d][sy][sx] = hv[d];
+  }
+  __syncthreads();
+  const bool xp = i + 1 < nx, xm = i > 0, yp = j + 1 < ny, ym = j > 0;
+  for (int k = k0; k < k1; ++k) {
+    const int b = (k - k0) & 1;
+    const bool next = k + 1 < k1;   // plane k+1 is this block's: the ring goes to shared memory
+    if (k + 1 < nz) {
+      if (own) {
+        av_col_vc<T>(oc, l, ex, ey, ez, vcm, flags, nc, sxk, syk, szk, s, own_hole, i, j, k + 1, f, vp);
+        if (next && (f & kFlagStoreVc)) {
+          const long long cell = l.cbase + ((long long)(k + 1) * ny + j) * nx + i;
+          vcm[cell] = vp[0];
+          vcm[nc + cell] = vp[1];
+          vcm[2 * nc + cell] = vp[2];
+        }
+      }
+      if (next && ring)
+        av_col_vc<T>(rc, l, ex, ey, ez, vcm, flags, nc, sxk, syk, szk, s, ring_hole, hi, hj, k + 1, f, hv);
+      if (next) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          sv[b ^ 1][d][ty + 1][tx + 1] = vp[d];
+          if (ring) sv[b ^ 1][d][sy][sx] = hv[d];
+        }
+      }
+    }
+    if (own && !(own_hole && k >= l.hole_lo[2] && k < l.hole_hi[2])) {
+      const bool zp = k + 1 < nz, zm = k > 0;
+      T* dst = vq + l.cbase + ((long long)k * ny + j) * nx + i;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const T x0 = v0[d];
+        T acc = 0;
+        acc += xp ? sv[b][d][ty + 1][tx + 2] - x0 : -2 * x0;
+        acc += xm ? sv[b][d][ty + 1][tx] - x0 : -2 * x0;
+        acc += yp ? sv[b][d][ty + 2][tx + 1] - x0 : -2 * x0;
+        acc += ym ? sv[b][d][ty][tx + 1] - x0 : -2 * x0;
+        acc += zp ? vp[d] - x0 : -2 * x0;
+        acc += zm ? vm[d] - x0 : -2 * x0;
+        dst[d * nc] = rou * x0 - kf * (acc * inv_h2);
+      }
+    }
+    if (next) __syncthreads();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      vm[d] = v0[d];
+      v0[d] = vp[d];
+    }
   }
 }
 
@@ -848,9 +1052,6 @@ constexpr size_t kFusedSmemBytes =
     (size_t)(kPRing * kPPlane + 2 * 3 * FY * FX + 3 * FY * FX + kMaxKzF * FY) * sizeof(double) +
     (size_t)kPPlane * sizeof(int);
 
-// cell flags of the fused matvec (one byte per cell)
-constexpr unsigned char kFlagExactVc = 1, kFlagExactVq = 2, kFlagStoreVq = 4;
-
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   const int n = ok ? 8 : 0;   // 0 source bytes: the 8 destination bytes are zero-filled
@@ -1193,6 +1394,16 @@ __global__ void __launch_bounds__(kThreads) k_vc_list(Meta m, long long n, const
   vcm[c] = vx;
   vcm[m.nc + c] = vy;
   vcm[2 * m.nc + c] = vz;
+}
+
+// setup: flags[c] |= bit for the listed cells
+__global__ void k_flag_list(long long n, const int* __restrict__ ids, long long nc, unsigned char bit,
+                            unsigned char* flags) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int c = ids[q];
+    if (c >= 0 && c < nc) flags[c] |= bit;
+  }
 }
 
 // setup: cell bits from a list of cell ids (or of component-major vq columns)
@@ -2337,9 +2548,12 @@ int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* 
   const Meta& m = sizeof(T) == 4 ? ctx->meta32 : ctx->meta;
   const long long nc = ctx->lay.ncell;
   const dim3 blk(TX, TY, 1), gA(m.gxA, m.gyA, m.gzA), gV(m.gxV, m.gyA, m.gzA), gR(m.gxR, m.gyR, m.gzR);
-  k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, pa_val, ctx->nA,
-                                        ctx->st);
-  CKL();
+  if (alpd && m.av && !ctx->flags_ready) return set_err(ctx, PYIB_E_STATE, "fused A+V kernel without its cell flags");
+  if (!(alpd && m.av)) {
+    k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, pa_val, ctx->nA,
+                                          ctx->st);
+    CKL();
+  }
   if (ctx->nA > 0) {
     k_patchA<T><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
         ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR), tp<int>(ctx, PYIB_T_PA_COL),
@@ -2347,7 +2561,19 @@ int launch_matvec_t(pyib_ctx* ctx, const T* in, T* out, T* vcm, T* vq, const T* 
     CKL();
   }
   const T* vsrc = vcm;
-  if (alpd) {
+  if (alpd && m.av) {
+    // exact vc rows (k_patchA, above) first, then vq = V P C p in one pass, then the
+    // exact vq rows
+    k_mvAV<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, vq, ctx->f_flags, ctx->st);
+    CKL();
+    if (ctx->nV > 0) {
+      k_patchV<T><<<patch_grid(ctx->nV), kThreads, 0, ctx->stream>>>(
+          ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR), tp<int>(ctx, PYIB_T_PV_COL),
+          pv_val, vcm, vq, nc, ctx->st);
+      CKL();
+    }
+    vsrc = vq;
+  } else if (alpd) {
     k_mvV<T><<<gV, blk, 0, ctx->stream>>>(m, vcm, vq, ctx->st);
     CKL();
     if (ctx->nV > 0) {
@@ -2377,8 +2603,8 @@ int launch_matvec(pyib_ctx* ctx, const double* in, double* out, int alpd, int do
 // Flags and lists of the fused matvec, from the patch tables (once per table upload):
 // irrA / irrV = cells with exact vc / vq rows, needR = cells whose vq an exact w row
 // reads, and the list of regular cells whose template vc an exact vq row reads.
-int prepare_fused(pyib_ctx* ctx) {
-  if (ctx->fused_ready) return PYIB_OK;
+int prepare_flags(pyib_ctx* ctx) {
+  if (ctx->flags_ready) return PYIB_OK;
   const long long nc = ctx->lay.ncell, words = (nc + 31) / 32;
   unsigned int** bits[] = {&ctx->f_irrA, &ctx->f_irrV, &ctx->f_needR};
   for (unsigned int** b : bits) {
@@ -2429,9 +2655,21 @@ int prepare_fused(pyib_ctx* ctx) {
     if (want[c]) list.push_back((int)c);
   ctx->n_list = (long long)list.size();
   RET(alloc(ctx, (void**)&ctx->f_list, std::max<size_t>(1, list.size()) * sizeof(int)));
-  if (!list.empty())
+  if (!list.empty()) {
     CK(cudaMemcpyAsync(ctx->f_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    k_flag_list<<<grid_for(ctx->n_list), kThreads, 0, ctx->stream>>>(ctx->n_list, ctx->f_list, nc, kFlagStoreVc,
+                                                                     ctx->f_flags);
+    CKL();
+  }
   CK(cudaStreamSynchronize(ctx->stream));
+  ctx->flags_ready = true;
+  return PYIB_OK;
+}
+
+// prepare_flags plus the single-pass kernel's reduction slots and shared memory
+int prepare_fused(pyib_ctx* ctx) {
+  if (ctx->fused_ready) return PYIB_OK;
+  RET(prepare_flags(ctx));
   if ((long long)ctx->meta.nplanesF + patch_grid(ctx->nR) > kPartStride)
     return set_err(ctx, PYIB_E_ARG, "too many reduction slots for the fused matvec");
   CK(cudaFuncSetAttribute(k_mvF, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemBytes));
@@ -2512,8 +2750,13 @@ int tune_fused(pyib_ctx* ctx) {
   return PYIB_OK;
 }
 
-// Autotuner: time the float64 matvec for every pair of z-chunk depths (cells, nodes)
-// and keep the fastest.  Runs once per context, before any CG graph is captured.
+// Matvec forms the autotuners try: kernels A and V as two kernels (0) and fused (1).
+// PYIB_MATVEC_AV=0 or =1 (read at context creation) pins one of them.
+int av_lo(const pyib_ctx* ctx) { return ctx->av_pin == 1 ? 1 : 0; }
+int av_hi(const pyib_ctx* ctx) { return ctx->av_pin == 0 ? 0 : 1; }
+
+// Autotuner: time the float64 matvec for every pair of z-chunk depths (cells, nodes),
+// with kernels A and V apart and fused, and keep the fastest.  Runs once per context, before any CG graph is captured.
 int tune_matvec(pyib_ctx* ctx) {
   if (ctx->tuned) return PYIB_OK;
   CGState h{};
@@ -2526,31 +2769,37 @@ int tune_matvec(pyib_ctx* ctx) {
   t.counter = 0u;
   CK(cudaMemcpyAsync(ctx->st, &t, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
   const int depths[5] = {1, 2, 4, 8, 16};
+  RET(prepare_flags(ctx));
   const Meta base = ctx->meta;
-  int bestA = base.kz, bestR = base.kzR;
+  int bestA = base.kz, bestR = base.kzR, bestAV = 0;
   double best = 1e30;
-  for (int a = 0; a < 5; ++a) {
-    for (int b = 0; b < 5; ++b) {
-      Meta m2 = base;
-      set_grids(m2, depths[a], depths[b]);
-      if ((long long)m2.gxR * m2.gyR * m2.gzR > kPartStride) continue;
-      ctx->meta = m2;
-      RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
-      CK(cudaEventRecord(ctx->ev0, ctx->stream));
-      for (int q = 0; q < 3; ++q) RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
-      CK(cudaEventRecord(ctx->ev1, ctx->stream));
-      CK(cudaEventSynchronize(ctx->ev1));
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-      if (ms < best) {
-        best = ms;
-        bestA = depths[a];
-        bestR = depths[b];
+  for (int av = av_lo(ctx); av <= av_hi(ctx); ++av) {
+    for (int a = 0; a < 5; ++a) {
+      for (int b = 0; b < 5; ++b) {
+        Meta m2 = base;
+        set_grids(m2, depths[a], depths[b]);
+        m2.av = av;
+        if ((long long)m2.gxR * m2.gyR * m2.gzR > kPartStride) continue;
+        ctx->meta = m2;
+        RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (int q = 0; q < 3; ++q) RET(launch_matvec(ctx, ctx->work_e, ctx->work_e2, 1, 0));
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        if (ms < best) {
+          best = ms;
+          bestA = depths[a];
+          bestR = depths[b];
+          bestAV = av;
+        }
       }
     }
   }
   ctx->meta = base;
   set_grids(ctx->meta, bestA, bestR);
+  ctx->meta.av = bestAV;
   ctx->tune_ms = best / 3.0;
   ctx->tuned = true;
   ctx->cg_graph_check = -1;
@@ -2577,35 +2826,41 @@ int tune_matvec32(pyib_ctx* ctx) {
   const long long ne = ctx->lay.nedge;
   CK(cudaMemsetAsync(ctx->p32, 0, ne * sizeof(float), ctx->stream));
   const int depths[5] = {1, 2, 4, 8, 16};
+  RET(prepare_flags(ctx));
   const Meta base = ctx->meta;
-  int bestA = base.kz, bestR = base.kzR;
+  int bestA = base.kz, bestR = base.kzR, bestAV = 0;
   double best = 1e30;
-  for (int a = 0; a < 5; ++a) {
-    for (int b = 0; b < 5; ++b) {
-      Meta m2 = base;
-      set_grids(m2, depths[a], depths[b]);
-      if ((long long)m2.gxR * m2.gyR * m2.gzR > kPartStride) continue;
-      ctx->meta32 = m2;
-      auto once = [&]() {
-        return launch_matvec_t<float>(ctx, ctx->p32, ctx->w32, ctx->vcm32, ctx->vq32, ctx->p32, 1, 0,
-                                      ctx->pa_val32, ctx->pv_val32, ctx->pr_val32);
-      };
-      RET(once());
-      CK(cudaEventRecord(ctx->ev0, ctx->stream));
-      for (int q = 0; q < 3; ++q) RET(once());
-      CK(cudaEventRecord(ctx->ev1, ctx->stream));
-      CK(cudaEventSynchronize(ctx->ev1));
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-      if (ms < best) {
-        best = ms;
-        bestA = depths[a];
-        bestR = depths[b];
+  for (int av = av_lo(ctx); av <= av_hi(ctx); ++av) {
+    for (int a = 0; a < 5; ++a) {
+      for (int b = 0; b < 5; ++b) {
+        Meta m2 = base;
+        set_grids(m2, depths[a], depths[b]);
+        m2.av = av;
+        if ((long long)m2.gxR * m2.gyR * m2.gzR > kPartStride) continue;
+        ctx->meta32 = m2;
+        auto once = [&]() {
+          return launch_matvec_t<float>(ctx, ctx->p32, ctx->w32, ctx->vcm32, ctx->vq32, ctx->p32, 1, 0,
+                                        ctx->pa_val32, ctx->pv_val32, ctx->pr_val32);
+        };
+        RET(once());
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (int q = 0; q < 3; ++q) RET(once());
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        if (ms < best) {
+          best = ms;
+          bestA = depths[a];
+          bestR = depths[b];
+          bestAV = av;
+        }
       }
     }
   }
   ctx->meta32 = base;
   set_grids(ctx->meta32, bestA, bestR);
+  ctx->meta32.av = bestAV;
   ctx->tuned32 = true;
   ctx->mix_graph_check = -1;
   CK(cudaMemcpyAsync(ctx->st, &h, sizeof(CGState), cudaMemcpyHostToDevice, ctx->stream));
@@ -2639,6 +2894,16 @@ int masked_matvec(pyib_ctx* ctx, const double* in, double* out, double dt, int a
     if (!(alpd & 1)) return set_err(ctx, PYIB_E_ARG, "the fused matvec needs the viscous block (alpd 3)");
     if (!ctx->tunedF) set_grids_fused(ctx->meta, ctx->meta.kzF > 0 ? ctx->meta.kzF : 16);
     return launch_matvec_fused(ctx, in, out, 0);
+  }
+  if (alpd & 12) {
+    // kernels A and V pinned: fused (4) or apart (8), viscous block on
+    if (!(alpd & 1)) return set_err(ctx, PYIB_E_ARG, "a pinned A/V form needs the viscous block (alpd 5 or 9)");
+    RET(prepare_flags(ctx));
+    const int keep = ctx->meta.av;
+    ctx->meta.av = (alpd & 4) ? 1 : 0;
+    const int rc = launch_matvec(ctx, in, out, 1, 0);
+    ctx->meta.av = keep;
+    return rc;
   }
   RET(launch_matvec(ctx, in, out, alpd, 0));
   return PYIB_OK;
@@ -3222,12 +3487,20 @@ int bench_matvec_t(pyib_ctx* ctx, int reps, const T* in, T* out, T* vcm, T* vq, 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int q = 0; q < reps; ++q) {
       switch (kern) {
-        case 0: k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                                      ctx->nA, ctx->st); break;
+        case 0:
+          if (m.av)
+            k_mvAV<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, vq, ctx->f_flags, ctx->st);
+          else
+            k_mvA<T><<<gA, blk, 0, ctx->stream>>>(m, in, vcm, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                  ctx->nA, ctx->st);
+          break;
         case 1: k_patchA<T><<<patch_grid(3 * ctx->nA), kThreads, 0, ctx->stream>>>(
                     ctx->nA, tp<int>(ctx, PYIB_T_PA_IDS), tp<long long>(ctx, PYIB_T_PA_PTR),
                     tp<int>(ctx, PYIB_T_PA_COL), pa, in, vcm, nc, ctx->st); break;
-        case 2: k_mvV<T><<<gV, blk, 0, ctx->stream>>>(m, vcm, vq, ctx->st); break;
+        case 2:
+          if (m.av) continue;   // fused into kernel AV (slot 1)
+          k_mvV<T><<<gV, blk, 0, ctx->stream>>>(m, vcm, vq, ctx->st);
+          break;
         case 3: k_patchV<T><<<patch_grid(ctx->nV), kThreads, 0, ctx->stream>>>(
                     ctx->nV, tp<int>(ctx, PYIB_T_PV_IDS), tp<long long>(ctx, PYIB_T_PV_PTR),
                     tp<int>(ctx, PYIB_T_PV_COL), pv, vcm, vq, nc, ctx->st); break;
@@ -3363,6 +3636,8 @@ int pyib_create(const pyib_layout* layout, pyib_ctx** out) {
   {
     const char* f = std::getenv("PYIB_FUSED_MATVEC");
     ctx->use_fused = f && f[0] == '1';
+    const char* av = std::getenv("PYIB_MATVEC_AV");
+    ctx->av_pin = (av && av[0] == '0') ? 0 : (av && av[0] == '1') ? 1 : -1;
   }
   {
     // default z-chunk depth: the deepest of 16, 8, 4, 2, 1 planes that still yields
@@ -3488,6 +3763,7 @@ int pyib_upload(pyib_ctx* ctx, int32_t table, const void* host, size_t bytes) {
   ctx->tuned32 = false;
   ctx->tunedF = false;
   ctx->fused_ready = false;
+  ctx->flags_ready = false;
   return PYIB_OK;
 }
 
@@ -3502,6 +3778,7 @@ int pyib_finalize(pyib_ctx* ctx, const int64_t* counts, int32_t ncounts) {
   ctx->tuned32 = false;
   ctx->tunedF = false;
   ctx->fused_ready = false;
+  ctx->flags_ready = false;
   if ((long long)ctx->meta.gxR * ctx->meta.gyR * ctx->meta.gzR + patch_grid(ctx->nR) > kPartStride ||
       (long long)ctx->meta.nplanes + patch_grid(ctx->nR) > kPartStride)
     return set_err(ctx, PYIB_E_ARG, "too many reduction slots for this layout");
@@ -3758,6 +4035,19 @@ int pyib_cg_timing(pyib_ctx* ctx, double* out, int32_t reset) {
     ctx->cg_seconds = 0.0;
     ctx->cg_iters = 0;
     ctx->launches = 0;
+  }
+  return PYIB_OK;
+}
+
+int pyib_matvec_plan(pyib_ctx* ctx, int32_t* out) {
+  if (!ctx || !out) return PYIB_E_ARG;
+  const Meta* ms[2] = {&ctx->meta, &ctx->meta32};
+  const bool tuned[2] = {ctx->tuned, ctx->tuned32};
+  for (int q = 0; q < 2; ++q) {
+    out[4 * q + 0] = tuned[q] ? 1 : 0;
+    out[4 * q + 1] = ms[q]->kz;
+    out[4 * q + 2] = ms[q]->kzR;
+    out[4 * q + 3] = ms[q]->av;
   }
   return PYIB_OK;
 }

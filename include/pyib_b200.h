@@ -176,7 +176,10 @@ int pyib_get_field(pyib_ctx* ctx, int32_t field, void* host, size_t count);
  * DirBC (ib_core_np.py:168-175, ib_driver_np.py:29-33) / Asp @ pp
  * (ib_driver_np.py:387).  alpd 1 selects the viscous block (0: without it);
  * alpd 3 computes the same product (viscous block on) with the single-pass fused
- * kernel the float64 CG uses, whose rows are bit-identical to the three-kernel path. */
+ * kernel the float64 CG uses, whose rows are bit-identical to the three-kernel path.
+ * alpd 5 and 9 pin the form of the curl+interp and viscous stencils (viscous block
+ * on): 5 runs them as one fused kernel, 9 as two kernels; both give the same bits,
+ * and alpd 1 uses whichever form the autotuner picked (two kernels before tuning). */
 int pyib_matvec(pyib_ctx* ctx, int32_t in_field, int32_t out_field, double dt, int32_t alpd);
 /* Single-component operators on the scratch fields:
  *  op 0: curl   WORK_E  -> WORK_F  (ib_core_np.py:133)
@@ -256,6 +259,11 @@ int pyib_diagnostics(pyib_ctx* ctx, double* out);
  * by this context, out[3] and out[4] the z-chunk depths of the cell and node
  * stencil tiles the autotuner picked (out holds 5 doubles). */
 int pyib_cg_timing(pyib_ctx* ctx, double* out, int32_t reset);
+/* The matvec plan the autotuner chose (benchmark support; the reference has no
+ * tiles to tune).  out holds 8 int32: for the float64 matvec, then the float32
+ * matvec of the mixed solver, each [tuned (0/1), cell-tile z depth, node-tile z
+ * depth, curl+interp and viscous templates fused (1) or two kernels (0)]. */
+int pyib_matvec_plan(pyib_ctx* ctx, int32_t* out);
 /* CUDA events on the context's stream: which=0 records the start, which=1 records
  * the end, waits for it and returns the elapsed milliseconds. */
 int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms);
@@ -263,7 +271,8 @@ int pyib_event(pyib_ctx* ctx, int32_t which, double* elapsed_ms);
  * events (benchmark support).  ms_per holds 7 doubles: [0] one matvec, then one
  * launch of each of its kernels alone: [1] curl+interp template, [2] its patch
  * rows, [3] viscous template, [4] its patch rows, [5] integr+rot template with the
- * dot, [6] its patch rows with the final reduction.  With params.precision = 1 the
+ * dot, [6] its patch rows with the final reduction.  When the tuned matvec runs the
+ * curl+interp and viscous templates as one kernel, [1] times that kernel and [3] is 0.  With params.precision = 1 the
  * float32 matvec of the mixed solver is timed instead (on a float32 copy of WORK_E). */
 int pyib_bench_matvec(pyib_ctx* ctx, int32_t reps, double dt, double* ms_per);
 
