@@ -807,11 +807,17 @@ def aggregate_batch(dist, seconds_concurrent, seconds_sequential, cells, launche
 
 
 def run_batch(args, world, rank, local):
-    """Aggregate cell-updates/s of the seeded sweep, concurrently and one case at a time.
+    """Aggregate cell-updates/s of the seeded sweep: batched (``value``: one
+    ``pyib_batch``, the CG iterations of all cases as one launch per kernel stage,
+    graph-captured), concurrently (one host thread and stream per case) and one
+    case at a time.
 
-    Both timings advance every case by ``--steps`` steps (consecutive steps of the
-    same runs: first concurrently, then sequentially); host wall clock around
-    each phase, every case's last call having waited for its own stream.  Under
+    Each timing advances every case by ``--steps`` steps (consecutive steps of the
+    same runs: batched, then concurrently, then sequentially); host wall clock
+    around each phase, every case's last call having waited for its own stream.
+    The batched phase also reports the CUDA-event time of its batched CG chunks
+    and their algorithmic HBM rate (80 B per edge and CG iteration, summed over
+    the cases) against the measured peak.  Under
     torchrun the cases are split across the ranks by cost (cells x steps,
     longest first, ``batch.partition``): each rank runs its own share with no
     collective on the data path, and the line reports the summed work over the
@@ -840,11 +846,17 @@ def run_batch(args, world, rank, local):
     sampler = ClockSampler(local if world > 1 else 0) if rank == 0 else None
     if sampler:
         sampler.start()
-    t_con, st_con = batch.advance(args.steps, concurrent=True) if mine else (0.0, {"cg_iterations": 0,
-                                                                               "max_case_iterations": 0})
+    empty = {"cg_iterations": 0, "max_case_iterations": 0, "per_case_iterations": []}
+    batch.batch_timing(reset=True)
+    t_bat, st_bat = batch.advance(args.steps, batched=True) if mine else (0.0, empty)
+    bt = batch.batch_timing(reset=True)
+    edges = [int(r.drv.layout.edge_exists.sum()) for r in batch.runs]
+    per_edge = ALGO_BYTES_PER_EDGE_ITER if args.precision == "float64" else ALGO_BYTES_PER_EDGE_ITER / 2
+    cg_bytes = float(sum(per_edge * e * it for e, it in zip(edges, st_bat["per_case_iterations"])))
     barrier(dist)
-    t_seq, st_seq = batch.advance(args.steps, concurrent=False) if mine else (0.0, {"cg_iterations": 0,
-                                                                                "max_case_iterations": 0})
+    t_con, st_con = batch.advance(args.steps, concurrent=True) if mine else (0.0, empty)
+    barrier(dist)
+    t_seq, st_seq = batch.advance(args.steps, concurrent=False) if mine else (0.0, empty)
     clocks = sampler.stop() if sampler else None
     launches = 0
     timing = (C.c_double * 5)()
@@ -853,6 +865,9 @@ def run_batch(args, world, rank, local):
         launches += int(timing[2])
     con = aggregate_batch(dist, t_con, t_seq, sum(cells), launches, st_con["cg_iterations"],
                           st_con["max_case_iterations"])
+    bat = aggregate_batch(dist, t_bat, bt["chunk_seconds"], sum(cells), bt["batched_launches"],
+                          st_bat["cg_iterations"], st_bat["max_case_iterations"])
+    bat_bytes = reduce_sum(dist, cg_bytes)
     seq = aggregate_batch(dist, t_con, t_seq, sum(cells), 0, st_seq["cg_iterations"],
                           st_seq["max_case_iterations"])
     batch.close()
@@ -861,10 +876,14 @@ def run_batch(args, world, rank, local):
     if rank != 0:
         return 0
     upd = con["cells"] * args.steps
+    peak, peak_kind = peaks()
+    # bat: seconds_concurrent = the batched phase's wall clock, seconds_sequential = its
+    # CUDA-event chunk time (max over ranks)
+    chunk_s = bat["seconds_sequential"]
     line = {
-        "metric": "batched sweep cell-updates/s", "value": upd / con["seconds_concurrent"],
+        "metric": "batched sweep cell-updates/s", "value": upd / bat["seconds_concurrent"],
         "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * con["seconds_concurrent"] / args.steps,
+        "ms_per_step": 1000.0 * bat["seconds_concurrent"] / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64" if args.precision == "float64" else "f32+f64", "data": "synthetic",
         "config": {"workload": "batched_sweep", "cases": len(cases), "seed": 0,
@@ -874,7 +893,18 @@ def run_batch(args, world, rank, local):
                    "setup_seconds": setup_s, "l2": "inputs larger than L2",
                    "parallelism": f"cases split over {world} GPU(s) by cells x steps",
                    "cells_per_rank": [int(x // args.steps) for x in loads]},
-        "concurrent": {"seconds": con["seconds_concurrent"], "cg_iterations": int(con["cg_iterations"]),
+        "batched": {"seconds": bat["seconds_concurrent"], "cg_iterations": int(bat["cg_iterations"]),
+                    "max_case_iterations": int(bat["max_case_iterations"]),
+                    "cg_chunk_seconds": chunk_s, "batched_kernel_launches": int(bat["launches"]),
+                    "graph_captures": int(bt["graph_captures"]),
+                    "roofline": {"bound": "hbm", "achieved": bat_bytes / max(chunk_s, 1e-12) / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": bat_bytes / max(chunk_s, 1e-12) / 1e9 / peak,
+                                 "peak_kind": peak_kind,
+                                 "algorithmic_bytes": bat_bytes,
+                                 "kernel": "batched CG iteration chunks (80 B per edge and iteration in "
+                                           "float64, 40 B in the float32 iterations of the mixed form; all cases)"}},
+        "concurrent": {"value": upd / con["seconds_concurrent"], "seconds": con["seconds_concurrent"],
+                       "cg_iterations": int(con["cg_iterations"]),
                        "max_case_iterations": int(con["max_case_iterations"])},
         "one_at_a_time": {"value": upd / seq["seconds_sequential"], "seconds": seq["seconds_sequential"],
                           "cg_iterations": int(seq["cg_iterations"]),

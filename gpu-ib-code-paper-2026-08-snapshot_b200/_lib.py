@@ -42,7 +42,8 @@ EXPORTS = [
     "pyib_operator", "pyib_calc_vel", "pyib_conv_diff", "pyib_helm_solve", "pyib_step",
     "pyib_ib_stencil", "pyib_ib_interp", "pyib_ib_spread", "pyib_loads", "pyib_diagnostics",
     "pyib_cg_timing", "pyib_matvec_plan", "pyib_event", "pyib_bench_matvec", "pyib_bench_matvec_fused", "pyib_spread_noalloc", "pyib_ib_interp_dx", "pyib_graph_pcg",
-    "pyib_recover_pressure",
+    "pyib_recover_pressure", "pyib_batch_create", "pyib_batch_destroy", "pyib_batch_last_error",
+    "pyib_batch_step", "pyib_batch_timing",
 ]
 
 
@@ -142,6 +143,12 @@ def load():
         "pyib_graph_pcg": [vp, C.c_int64, vp, vp, vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
                            C.POINTER(C.c_double)],
         "pyib_recover_pressure": [vp, C.c_int64, vp, C.c_int64, vp, vp, vp, C.c_double, C.c_int32, vp, vp],
+        "pyib_batch_create": [C.POINTER(vp), C.c_int32, C.POINTER(vp)],
+        "pyib_batch_destroy": [vp],
+        "pyib_batch_last_error": [vp, C.c_char_p, C.c_size_t],
+        "pyib_batch_step": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32, C.POINTER(vp),
+                            C.POINTER(vp), C.POINTER(StepStats)],
+        "pyib_batch_timing": [vp, C.POINTER(C.c_double), C.c_int32],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -213,3 +220,38 @@ class Handle:
         out = np.empty(int(count), dtype=dtype)
         self.call("pyib_get_field", F[name], out.ctypes.data_as(C.c_void_p), out.size)
         return out
+
+
+class Batch:
+    """Owner of one ``pyib_batch`` over the contexts of ``handles`` (which it does not own)."""
+
+    def __init__(self, handles):
+        self.lib = load()
+        self.handles = list(handles)
+        arr = (C.c_void_p * len(self.handles))(*[h.ptr.value for h in self.handles])
+        self.ptr = C.c_void_p()
+        rc = self.lib.pyib_batch_create(arr, len(self.handles), C.byref(self.ptr))
+        if rc != OK:
+            raise B200Error(rc, "pyib_batch_create: " + self.handles[0].error())
+
+    def error(self):
+        buf = C.create_string_buffer(1024)
+        self.lib.pyib_batch_last_error(self.ptr, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def call(self, name, *args):
+        rc = getattr(self.lib, name)(self.ptr, *args)
+        if rc != OK:
+            raise B200Error(rc, f"{name}: {self.error()}")
+        return rc
+
+    def close(self):
+        if self.ptr:
+            self.lib.pyib_batch_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

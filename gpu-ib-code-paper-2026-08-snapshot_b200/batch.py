@@ -1,12 +1,19 @@
 """Batched sweep: many independent oscillating-sphere cases of uneven size on one GPU.
 
 Each case is a full ``SphereRun`` (its own library context, CUDA stream, CG
-graphs and autotuned tiles).  ``BatchRun.advance`` drives every case from its
-own host thread -- one context per host thread, as the C ABI requires -- so the
-cases' graph replays and kernels run concurrently on their streams and fill
-the gaps a single case leaves (host polls every ``check`` iterations, the tail
-blocks of small grids, launch latency of the patch kernels).  The library
-calls release the Python interpreter lock (ctypes), so the threads overlap.
+graphs and autotuned tiles).  ``BatchRun.advance`` steps the cases in one of
+three ways:
+
+* batched: one ``pyib_batch`` over all contexts; each step runs every case's
+  step parts on its own stream, and the CG iterations of all cases' Helmholtz
+  solves run together, one launch per kernel stage over the tiles of every case
+  still iterating, ``check`` iterations to one CUDA graph;
+* concurrent: every case from its own host thread (one context per host thread),
+  so the cases' graph replays and kernels overlap on their streams; the library
+  calls release the Python interpreter lock (ctypes);
+* one case after the other.
+
+All three give every case the same bits.
 
 Cases with the same resolution share one ``LayoutTables`` (operators, masks,
 patch rows), built once on the host.
@@ -26,8 +33,9 @@ from collections import Counter
 import numpy as np
 
 from .cases import SphereCase
+from . import _lib
 from .device import LayoutTables
-from .runner import SphereRun
+from .runner import SphereRun, advance_batch
 
 SWEEP_CELLS_PER_DIAMETER = (12, 16, 20, 24, 32)
 
@@ -83,6 +91,7 @@ class BatchRun:
         self.cases = list(cases)
         self.tables = {}
         self.runs = []
+        self._batch = None
         for c in self.cases:
             key = (c.cells_per_diameter, tuple(c.half_widths_d), bool(c.cavity))
             if key not in self.tables:
@@ -109,12 +118,27 @@ class BatchRun:
 
     def _stats(self, per_run_iters):
         return {"cg_iterations": int(sum(sum(x) for x in per_run_iters)),
-                "max_case_iterations": int(max(sum(x) for x in per_run_iters))}
+                "max_case_iterations": int(max(sum(x) for x in per_run_iters)),
+                "per_case_iterations": [int(sum(x)) for x in per_run_iters]}
 
-    def advance(self, steps=1, concurrent=True):
-        """Advance every case by ``steps`` steps; returns (seconds, stats)."""
+    def advance(self, steps=1, concurrent=True, batched=False):
+        """Advance every case by ``steps`` steps; returns (seconds, stats).
+
+        ``batched``: every step of all cases goes through one ``pyib_batch`` (the CG
+        iterations of all cases as one launch per kernel stage); otherwise each case
+        steps on its own context, from its own host thread (``concurrent``) or one
+        case after the other."""
         iters = [[] for _ in self.runs]
         errors = []
+        if batched:
+            if self._batch is None:
+                self._batch = _lib.Batch([r.drv.solver.h for r in self.runs])
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                advance_batch(self._batch, self.runs)
+                for q, r in enumerate(self.runs):
+                    iters[q].append(r.drv.helmholtz_total_iterations_last_step)
+            return time.perf_counter() - t0, self._stats(iters)
 
         def work(q):
             r = self.runs[q]
@@ -143,8 +167,20 @@ class BatchRun:
             raise RuntimeError(f"case {self.cases[q].name} failed: {exc}") from exc
         return seconds, self._stats(iters)
 
+    def batch_timing(self, reset=True):
+        """CUDA-event seconds of the batched CG chunks, batched kernels launched and
+        graph captures since the last reset (pyib_batch_timing)."""
+        import ctypes as C
+        out = (C.c_double * 3)()
+        if self._batch is not None:
+            self._batch.call("pyib_batch_timing", out, int(reset))
+        return {"chunk_seconds": out[0], "batched_launches": int(out[1]), "graph_captures": int(out[2])}
+
     def close(self):
-        """Release every case's device context."""
+        """Release the batch and every case's device context."""
+        if self._batch is not None:
+            self._batch.close()
+            self._batch = None
         for r in self.runs:
             if r.drv._solver is not None:
                 r.drv._solver.h.close()

@@ -263,15 +263,28 @@ __device__ __forceinline__ double strided_sum(const double* partials, int n) {
   return (a0 + a1) + (a2 + a3);
 }
 
-// Writes this block's partials; returns true in the block that finishes last,
-// whose thread 0 then holds the totals in v (summed in block order).
+// Block coordinates of a kernel body: the launch's own (blockIdx, gridDim), or, in a
+// batched launch over several cases, the block's coordinates within its case's grid.
+struct Grid3 {
+  int bx, by, bz, gx, gy, gz;
+};
+struct Grid1 {
+  int b, nb;   // block and block count of a one-dimensional grid
+};
+__device__ __forceinline__ Grid3 own_grid3() {
+  return Grid3{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)gridDim.x, (int)gridDim.y, (int)gridDim.z};
+}
+__device__ __forceinline__ Grid1 own_grid1() { return Grid1{(int)blockIdx.x, (int)gridDim.x}; }
+
+// Writes this block's partials; returns true in the block that finishes last (of the
+// nb blocks counted on counter), whose thread 0 then holds the totals in v (summed
+// in block order).
 template <int NV>
-__device__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counter) {
+__device__ bool grid_sum_at(double (&v)[NV], double* partials, unsigned int* counter, unsigned int bid,
+                            unsigned int nb) {
   __shared__ double sh[NV * 32];
   __shared__ bool last;
   block_sum<NV>(v, sh);
-  const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
-  const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nthr = blockDim.x * blockDim.y * blockDim.z;
   if (tid == 0) {
@@ -295,6 +308,12 @@ __device__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counte
     *counter = 0u;
   }
   return tid == 0;
+}
+
+template <int NV>
+__device__ bool grid_sum(double (&v)[NV], double* partials, unsigned int* counter) {
+  return grid_sum_at<NV>(v, partials, counter, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                         gridDim.x * gridDim.y * gridDim.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -365,20 +384,13 @@ void set_grids_fused(Meta& m, int kzF) {
 // Irregular cells (hole neighbours, interface cells) take their exact CSR rows.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p, T* __restrict__ vc,
-                                                  const unsigned int* __restrict__ pbits,
-                                                  const int* __restrict__ prow,
-                                                  const long long* __restrict__ pptr,
-                                                  const int* __restrict__ pcol,
-                                                  const T* __restrict__ pval, long long nA,
-                                                  const CGState* __restrict__ st) {
-  if (st && st->done) return;
-  const int L = level_of_zblock(m, blockIdx.z, false);
+__device__ __forceinline__ void mvA_tile(const Meta& m, Grid3 g, const T* __restrict__ p, T* __restrict__ vc) {
+  const int L = level_of_zblock(m, g.bz, false);
   const LevelMeta& l = m.lv[L];
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
-  const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
+  const int i = g.bx * TX + threadIdx.x, j = g.by * TY + threadIdx.y;
   if (i >= nx || j >= ny) return;
-  const int k0 = (blockIdx.z - l.zbA) * m.kz;
+  const int k0 = (g.bz - l.zbA) * m.kz;
   const int k1 = min(k0 + m.kz, nz);
   const long long nc = m.nc;
   const T* ex = p + l.ebase[0];
@@ -415,6 +427,18 @@ __global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p, T* __restrict__ vc,
+                                                  const unsigned int* __restrict__ pbits,
+                                                  const int* __restrict__ prow,
+                                                  const long long* __restrict__ pptr,
+                                                  const int* __restrict__ pcol,
+                                                  const T* __restrict__ pval, long long nA,
+                                                  const CGState* __restrict__ st) {
+  if (st && st->done) return;
+  mvA_tile<T>(m, own_grid3(), p, vc);
+}
+
 // ---------------------------------------------------------------------------
 // matvec kernel V: vq = rou v - kfac * Vd v per component (7-point template with a
 // zero ghost at the domain boundary).  Each thread owns two x-consecutive cells
@@ -423,16 +447,15 @@ __global__ void __launch_bounds__(TX * TY) k_mvA(Meta m, const T* __restrict__ p
 // irregular cells are overwritten by k_patchV.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v, T* __restrict__ vq,
-                                                  const CGState* __restrict__ st) {
-  if (st->done) return;
-  const int L = level_of_zblock(m, blockIdx.z, false);
+__device__ __forceinline__ void mvV_tile(const Meta& m, Grid3 g, const T* __restrict__ v, T* __restrict__ vq,
+                                         const CGState* __restrict__ st) {
+  const int L = level_of_zblock(m, g.bz, false);
   const LevelMeta& l = m.lv[L];
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
-  const int i = blockIdx.x * (2 * TX) + 2 * threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
+  const int i = g.bx * (2 * TX) + 2 * threadIdx.x, j = g.by * TY + threadIdx.y;
   if (i >= nx || j >= ny) return;
   const bool hasB = i + 1 < nx;                   // the second cell (i+1, j)
-  const int k0 = (blockIdx.z - l.zbA) * m.kz;
+  const int k0 = (g.bz - l.zbA) * m.kz;
   const int k1 = min(k0 + m.kz, nz);
   const long long nc = m.nc;
   const T rou = (T)st->rou, kf = (T)st->kfac;
@@ -490,6 +513,13 @@ __global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v
     src += cs;
     dst += cs;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY) k_mvV(Meta m, const T* __restrict__ v, T* __restrict__ vq,
+                                                  const CGState* __restrict__ st) {
+  if (st->done) return;
+  mvV_tile<T>(m, own_grid3(), v, vq, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -793,18 +823,16 @@ __device__ __forceinline__ double ri_plane(const LevelMeta& l, int i, int j, int
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
-                                                   const T* __restrict__ p,
-                                                   const unsigned int* __restrict__ pbits, double* partials,
-                                                   CGState* st, int do_dot) {
-  if (st->done) return;
+__device__ __forceinline__ void mvRI_tile(const Meta& m, Grid3 g, const T* __restrict__ vq, T* __restrict__ w,
+                                          const T* __restrict__ p, const unsigned int* __restrict__ pbits,
+                                          double* partials, int do_dot) {
   static_assert(TY == 8, "the per-plane combine below assumes 8 warps per block");
   __shared__ double swarp[16][TY];
-  const int L = level_of_zblock(m, blockIdx.z, true);
+  const int L = level_of_zblock(m, g.bz, true);
   const LevelMeta& l = m.lv[L];
   const int nx = l.n[0], ny = l.n[1], nz = l.n[2];
-  const int i = blockIdx.x * TX + threadIdx.x, j = blockIdx.y * TY + threadIdx.y;
-  const int k0 = (blockIdx.z - l.zbR) * m.kzR;
+  const int i = g.bx * TX + threadIdx.x, j = g.by * TY + threadIdx.y;
+  const int k0 = (g.bz - l.zbR) * m.kzR;
   const int k1 = min(k0 + m.kzR, nz + m.ri_up);
   const long long nc = m.nc;
   const T* vx = vq + l.cbase;
@@ -831,8 +859,17 @@ __global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ 
   if (tid < k1 - k0) {
     const double* q = swarp[tid];
     const double v = ((q[0] + q[4]) + (q[2] + q[6])) + ((q[1] + q[5]) + (q[3] + q[7]));
-    partials[l.plane_base + ((k0 + tid) * m.gyR + blockIdx.y) * m.gxR + blockIdx.x] = v;
+    partials[l.plane_base + ((k0 + tid) * m.gyR + g.by) * m.gxR + g.bx] = v;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY) k_mvRI(Meta m, const T* __restrict__ vq, T* __restrict__ w,
+                                                   const T* __restrict__ p,
+                                                   const unsigned int* __restrict__ pbits, double* partials,
+                                                   CGState* st, int do_dot) {
+  if (st->done) return;
+  mvRI_tile<T>(m, own_grid3(), vq, w, p, pbits, partials, do_dot);
 }
 
 // ---------------------------------------------------------------------------
@@ -870,27 +907,33 @@ __device__ __forceinline__ T csr_row(const long long* __restrict__ ptr, const in
 
 // vc rows: row q = d*nA + r holds component d of cell ids[r]
 template <typename T>
+__device__ __forceinline__ void patchA_rows(Grid1 g, long long nA, const int* __restrict__ ids,
+                                            const long long* __restrict__ ptr, const int* __restrict__ col,
+                                            const T* __restrict__ val, const T* __restrict__ p, T* vc,
+                                            long long nc) {
+  const long long q = g.b * (long long)blockDim.x + threadIdx.x;
+  if (q >= 3 * nA) return;
+  vc[(q / nA) * nc + ids[q % nA]] = csr_row<T>(ptr, col, val, p, q);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_patchA(long long nA, const int* __restrict__ ids,
                                                      const long long* __restrict__ ptr,
                                                      const int* __restrict__ col, const T* __restrict__ val,
                                                      const T* __restrict__ p, T* vc, long long nc,
                                                      const CGState* __restrict__ st) {
   if (st->done) return;
-  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (q >= 3 * nA) return;
-  vc[(q / nA) * nc + ids[q % nA]] = csr_row<T>(ptr, col, val, p, q);
+  patchA_rows<T>(own_grid1(), nA, ids, ptr, col, val, p, vc, nc);
 }
 
 // vq rows: the same Vd row for the three components of cell ids[r], one thread per row
 // (the row's columns and values are loaded once for the three gathers)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __restrict__ ids,
-                                                     const long long* __restrict__ ptr,
-                                                     const int* __restrict__ col, const T* __restrict__ val,
-                                                     const T* __restrict__ v, T* vq, long long nc,
-                                                     const CGState* __restrict__ st) {
-  if (st->done) return;
-  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void patchV_rows(Grid1 g, long long nV, const int* __restrict__ ids,
+                                            const long long* __restrict__ ptr, const int* __restrict__ col,
+                                            const T* __restrict__ val, const T* __restrict__ v, T* vq, long long nc,
+                                            const CGState* __restrict__ st) {
+  const long long r = g.b * (long long)blockDim.x + threadIdx.x;
   if (r >= nV) return;
   const int c = ids[r];
   const long long q0 = ptr[r], q1 = ptr[r + 1];
@@ -926,17 +969,26 @@ __global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __
   vq[2 * nc + c] = rou * v[2 * nc + c] - kf * a2;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_patchV(long long nV, const int* __restrict__ ids,
+                                                     const long long* __restrict__ ptr,
+                                                     const int* __restrict__ col, const T* __restrict__ val,
+                                                     const T* __restrict__ v, T* vq, long long nc,
+                                                     const CGState* __restrict__ st) {
+  if (st->done) return;
+  patchV_rows<T>(own_grid1(), nV, ids, ptr, col, val, v, vq, nc, st);
+}
+
 // w rows (columns index the component-major vq), plus their share of p.w; the
 // per-plane partials of k_mvRI and the rows' shares are summed in a fixed order
 // (independent of the z-chunk depth) and the last block sets alpha = eta / p.w.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* __restrict__ ids,
-                                                      const long long* __restrict__ ptr,
-                                                      const int* __restrict__ col, const T* __restrict__ val,
-                                                      const T* __restrict__ vq, T* w, const T* __restrict__ p,
-                                                      double* partials, int nplanes, CGState* st, int do_dot) {
-  if (st->done) return;
-  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void patchRI_rows(Grid1 g, long long nR, const int* __restrict__ ids,
+                                             const long long* __restrict__ ptr, const int* __restrict__ col,
+                                             const T* __restrict__ val, const T* __restrict__ vq, T* w,
+                                             const T* __restrict__ p, double* partials, int nplanes, CGState* st,
+                                             int do_dot) {
+  const long long r = g.b * (long long)blockDim.x + threadIdx.x;
   double dot[1] = {0.0};
   if (r < nR) {
     const int e = ids[r];
@@ -949,26 +1001,36 @@ __global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* _
   __shared__ bool last;
   // Two-stage fixed-order sum: each block adds a fixed slice of k_mvRI's per-plane
   // partials to its own rows' share, and the last block sums one value per block.
-  const int per = (nplanes + (int)gridDim.x - 1) / (int)gridDim.x;
-  const int q0 = min(nplanes, (int)blockIdx.x * per), q1 = min(nplanes, q0 + per);
+  const int per = (nplanes + g.nb - 1) / g.nb;
+  const int q0 = min(nplanes, g.b * per), q1 = min(nplanes, q0 + per);
   double v2[2] = {dot[0], 0.0};
   for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) v2[1] += partials[q];
   block_sum<2>(v2, sh);
   if (threadIdx.x == 0) {
-    partials[nplanes + blockIdx.x] = v2[0] + v2[1];
+    partials[nplanes + g.b] = v2[0] + v2[1];
     __threadfence();
-    last = atomicAdd(&st->counter, 1u) == gridDim.x - 1;
+    last = atomicAdd(&st->counter, 1u) == (unsigned int)g.nb - 1;
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
-  double acc[1] = {strided_sum(partials + nplanes, (int)gridDim.x)};
+  double acc[1] = {strided_sum(partials + nplanes, g.nb)};
   block_sum<1>(acc, sh);
   if (threadIdx.x == 0) {
     st->pw = acc[0];
     st->alpha = st->eta / (acc[0] != 0.0 ? acc[0] : INFINITY);
     st->counter = 0u;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_patchRI(long long nR, const int* __restrict__ ids,
+                                                      const long long* __restrict__ ptr,
+                                                      const int* __restrict__ col, const T* __restrict__ val,
+                                                      const T* __restrict__ vq, T* w, const T* __restrict__ p,
+                                                      double* partials, int nplanes, CGState* st, int do_dot) {
+  if (st->done) return;
+  patchRI_rows<T>(own_grid1(), nR, ids, ptr, col, val, vq, w, p, partials, nplanes, st, do_dot);
 }
 
 // ---------------------------------------------------------------------------
@@ -1461,18 +1523,16 @@ __device__ __forceinline__ double prec_of(const Meta& m, const unsigned int* __r
 
 // r -= alpha w on unmasked edges; eta' = sum (r*prec)*r; the last block applies the
 // stopping test (every `check` iterations, or at cg_max) and sets `stop`.
-__global__ void __launch_bounds__(kThreads, 8) k_cg_update(Meta m, long long ne, double* r,
-                                                        const double* __restrict__ w,
-                                                        const unsigned int* __restrict__ pbits,
-                                                        const double* __restrict__ prec,
-                                                        double* partials, CGState* st) {
-  if (st->done) return;
+__device__ __forceinline__ void cg_update_blocks(Grid1 g, const Meta& m, long long ne, double* r,
+                                                 const double* __restrict__ w,
+                                                 const unsigned int* __restrict__ pbits,
+                                                 const double* __restrict__ prec, double* partials, CGState* st) {
   const double alpha = st->alpha;
   double v[1] = {0.0};
   // two elements of the thread's grid-stride sequence per pass, loads first (more
   // bytes in flight); each element is computed and summed in the original order
-  const long long S = (long long)gridDim.x * blockDim.x;
-  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long S = (long long)g.nb * blockDim.x;
+  long long e = g.b * (long long)blockDim.x + threadIdx.x;
   for (; e + S < ne; e += 2 * S) {
     double pr[2], rv[2], wv[2];
 #pragma unroll
@@ -1497,7 +1557,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_cg_update(Meta m, long long ne,
       v[0] += (re * pr) * re;
     }
   }
-  if (grid_sum<1>(v, partials, &st->counter)) {
+  if (grid_sum_at<1>(v, partials, &st->counter, g.b, g.nb)) {
     const double en = v[0];
     st->eta_new = en;
     const int mm = st->m + 1;
@@ -1517,17 +1577,24 @@ __global__ void __launch_bounds__(kThreads, 8) k_cg_update(Meta m, long long ne,
   }
 }
 
+__global__ void __launch_bounds__(kThreads, 8) k_cg_update(Meta m, long long ne, double* r,
+                                                        const double* __restrict__ w,
+                                                        const unsigned int* __restrict__ pbits,
+                                                        const double* __restrict__ prec,
+                                                        double* partials, CGState* st) {
+  if (st->done) return;
+  cg_update_blocks(own_grid1(), m, ne, r, w, pbits, prec, partials, st);
+}
+
 // x += alpha p (the iterate of this iteration), then p = r*prec + beta p unless the
 // stopping test fired; the last block turns `stop` into `done`.
-__global__ void __launch_bounds__(kThreads) k_cg_p(Meta m, long long ne, const double* __restrict__ r,
-                                                   const unsigned int* __restrict__ pbits,
-                                                   const double* __restrict__ prec, double* p, double* x,
-                                                   CGState* st) {
-  if (st->done) return;
+__device__ __forceinline__ void cg_p_blocks(Grid1 g, const Meta& m, long long ne, const double* __restrict__ r,
+                                            const unsigned int* __restrict__ pbits,
+                                            const double* __restrict__ prec, double* p, double* x, CGState* st) {
   const double alpha = st->alpha, beta = st->beta;
   const bool stop = st->stop != 0;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x) {
+  for (long long e = g.b * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)g.nb * blockDim.x) {
     const double pe = p[e];
     x[e] += alpha * pe;
     if (!stop) p[e] = r[e] * prec_of(m, pbits, prec, e) + beta * pe;
@@ -1537,13 +1604,21 @@ __global__ void __launch_bounds__(kThreads) k_cg_p(Meta m, long long ne, const d
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned int t = atomicAdd(&st->counter2, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == (unsigned int)g.nb - 1);
   }
   __syncthreads();
   if (last && threadIdx.x == 0) {
     st->counter2 = 0u;
     if (stop) st->done = 1;
   }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cg_p(Meta m, long long ne, const double* __restrict__ r,
+                                                   const unsigned int* __restrict__ pbits,
+                                                   const double* __restrict__ prec, double* p, double* x,
+                                                   CGState* st) {
+  if (st->done) return;
+  cg_p_blocks(own_grid1(), m, ne, r, pbits, prec, p, x, st);
 }
 
 __global__ void k_mask(long long n, const double* __restrict__ prec, double* w) {
@@ -1612,16 +1687,13 @@ __global__ void __launch_bounds__(kThreads) k_mix_start(long long ne, const doub
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_cg_update32(long long ne, float* d32, float* r32,
-                                                          const float* __restrict__ p32,
-                                                          const float* __restrict__ w32,
-                                                          const float* __restrict__ dinv,
-                                                          double* partials, CGState* st) {
-  if (st->done) return;
+__device__ __forceinline__ void cg_update32_blocks(Grid1 g, long long ne, float* d32, float* r32,
+                                                   const float* __restrict__ p32, const float* __restrict__ w32,
+                                                   const float* __restrict__ dinv, double* partials, CGState* st) {
   const float alpha = (float)st->alpha;
   double v[1] = {0.0};
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
-       e += (long long)gridDim.x * blockDim.x) {
+  for (long long e = g.b * (long long)blockDim.x + threadIdx.x; e < ne;
+       e += (long long)g.nb * blockDim.x) {
     const float di = dinv[e];
     if (di != 0.f) {
       d32[e] += alpha * p32[e];
@@ -1630,7 +1702,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_update32(long long ne, float* d
       v[0] += (double)(re * di) * (double)re;
     }
   }
-  if (grid_sum<1>(v, partials, &st->counter)) {
+  if (grid_sum_at<1>(v, partials, &st->counter, g.b, g.nb)) {
     const double en = v[0];
     const int m = st->m + 1;
     st->m = m;
@@ -1647,13 +1719,20 @@ __global__ void __launch_bounds__(kThreads) k_cg_update32(long long ne, float* d
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 8) k_cg_p32(long long ne, const float* __restrict__ r32,
-                                                     const float* __restrict__ dinv, float* p32,
-                                                     const CGState* st) {
+__global__ void __launch_bounds__(kThreads) k_cg_update32(long long ne, float* d32, float* r32,
+                                                          const float* __restrict__ p32,
+                                                          const float* __restrict__ w32,
+                                                          const float* __restrict__ dinv,
+                                                          double* partials, CGState* st) {
   if (st->done) return;
+  cg_update32_blocks(own_grid1(), ne, d32, r32, p32, w32, dinv, partials, st);
+}
+
+__device__ __forceinline__ void cg_p32_blocks(Grid1 g, long long ne, const float* __restrict__ r32,
+                                              const float* __restrict__ dinv, float* p32, const CGState* st) {
   const float beta = (float)st->beta;
-  const long long S = (long long)gridDim.x * blockDim.x;
-  long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long S = (long long)g.nb * blockDim.x;
+  long long e = g.b * (long long)blockDim.x + threadIdx.x;
   for (; e + 3 * S < ne; e += 4 * S) {
     float rv[4], dv[4], pv[4];
 #pragma unroll
@@ -1666,6 +1745,13 @@ __global__ void __launch_bounds__(kThreads, 8) k_cg_p32(long long ne, const floa
     for (int u = 0; u < 4; ++u) p32[e + u * S] = rv[u] * dv[u] + beta * pv[u];
   }
   for (; e < ne; e += S) p32[e] = r32[e] * dinv[e] + beta * p32[e];
+}
+
+__global__ void __launch_bounds__(kThreads, 8) k_cg_p32(long long ne, const float* __restrict__ r32,
+                                                     const float* __restrict__ dinv, float* p32,
+                                                     const CGState* st) {
+  if (st->done) return;
+  cg_p32_blocks(own_grid1(), ne, r32, dinv, p32, st);
 }
 
 // Reliable update of the float32 CG: r32 = float(r64) (the float64 residual after
@@ -1761,9 +1847,125 @@ __global__ void k_dinv(long long ne, const double* __restrict__ d1, const double
 }
 
 // ---------------------------------------------------------------------------
-// Jacobi-preconditioned CG on a caller's CSR matrix (the offline pressure
-// recovery's graph Laplacian, ib_postprocess.py:49-107).  Deterministic sums.
+// Batched CG iterations: every stage of one iteration (matvec kernels A, V, RI with
+// their exact rows, the residual update and the direction update) is one launch over
+// the tiles of all cases of a batch.  Block b of a stage reads blk[b] = (case, block
+// within that case's grid) and runs the single-case body with those coordinates, so
+// every case computes exactly what its own kernels compute.  A case whose solve has
+// stopped (st->done) leaves its blocks idle; the host drops it from the tables.
 // ---------------------------------------------------------------------------
+constexpr int kBStages = 8;
+constexpr int kBatchCellDepth = 8, kBatchNodeDepth = 16;   // z planes of a batched cell / node tile
+constexpr int kBatchGroups = 4;   // cost-balanced groups of cases, parallel branches of the chunk graph
+
+struct BCase {
+  Meta m;                          // the case's layout decoding and tiles, of the batch's precision
+  CGState* st;
+  double* partials;
+  void *p, *w, *vcm, *vq, *r, *x;  // the CG vectors in the batch's precision (x: the float32 correction)
+  const void *pa_val, *pv_val, *pr_val;
+  const int *pa_ids, *pa_col, *pv_ids, *pv_col, *pr_ids, *pr_col;
+  const long long *pa_ptr, *pv_ptr, *pr_ptr;
+  const unsigned int *prec_bits, *pr_bits;
+  const double* prec;              // float64 preconditioner exceptions
+  const float* dinv;               // float32 Jacobi (mixed solver)
+  long long nA, nV, nR, ne, nc;
+  int nblk[kBStages];              // the case's blocks in each stage (its single-case grids)
+};
+
+__device__ __forceinline__ Grid3 batch_grid3(int lb, int gx, int gy, int gz) {
+  return Grid3{lb % gx, (lb / gx) % gy, lb / (gx * gy), gx, gy, gz};
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY) k_bA(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  const Meta& m = q.m;
+  mvA_tile<T>(m, batch_grid3(cb.y, m.gxA, m.gyA, m.gzA), (const T*)q.p, (T*)q.vcm);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bpatchA(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  patchA_rows<T>(Grid1{cb.y, q.nblk[1]}, q.nA, q.pa_ids, q.pa_ptr, q.pa_col, (const T*)q.pa_val, (const T*)q.p,
+                 (T*)q.vcm, q.nc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY, 4) k_bV(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  const Meta& m = q.m;
+  mvV_tile<T>(m, batch_grid3(cb.y, m.gxV, m.gyA, m.gzA), (const T*)q.vcm, (T*)q.vq, q.st);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bpatchV(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  patchV_rows<T>(Grid1{cb.y, q.nblk[3]}, q.nV, q.pv_ids, q.pv_ptr, q.pv_col, (const T*)q.pv_val,
+                 (const T*)q.vcm, (T*)q.vq, q.nc, q.st);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TX * TY) k_bRI(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  const Meta& m = q.m;
+  mvRI_tile<T>(m, batch_grid3(cb.y, m.gxR, m.gyR, m.gzR), (const T*)q.vq, (T*)q.w, (const T*)q.p, q.pr_bits,
+               q.partials, 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bpatchRI(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  patchRI_rows<T>(Grid1{cb.y, q.nblk[5]}, q.nR, q.pr_ids, q.pr_ptr, q.pr_col, (const T*)q.pr_val,
+                  (const T*)q.vq, (T*)q.w, (const T*)q.p, q.partials, q.m.nplanes, q.st, 1);
+}
+
+// float64 residual update and direction (k_cg_update, k_cg_p)
+__global__ void __launch_bounds__(kThreads, 8) k_bupdate(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  cg_update_blocks(Grid1{cb.y, q.nblk[6]}, q.m, q.ne, (double*)q.r, (const double*)q.w, q.prec_bits, q.prec,
+                   q.partials, q.st);
+}
+
+__global__ void __launch_bounds__(kThreads, 8) k_bdir(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  cg_p_blocks(Grid1{cb.y, q.nblk[7]}, q.m, q.ne, (const double*)q.r, q.prec_bits, q.prec, (double*)q.p,
+              (double*)q.x, q.st);
+}
+
+// float32 residual update and direction of the mixed solver (k_cg_update32, k_cg_p32)
+__global__ void __launch_bounds__(kThreads, 8) k_bupdate32(const BCase* __restrict__ cs,
+                                                           const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  cg_update32_blocks(Grid1{cb.y, q.nblk[6]}, q.ne, (float*)q.x, (float*)q.r, (const float*)q.p,
+                     (const float*)q.w, q.dinv, q.partials, q.st);
+}
+
+__global__ void __launch_bounds__(kThreads, 8) k_bdir32(const BCase* __restrict__ cs, const int2* __restrict__ blk) {
+  const int2 cb = blk[blockIdx.x];
+  const BCase& q = cs[cb.x];
+  if (q.st->done) return;
+  cg_p32_blocks(Grid1{cb.y, q.nblk[7]}, q.ne, (const float*)q.r, q.dinv, (float*)q.p, q.st);
+}
+
 struct GState {
   double rz, rr, bb, atol, alpha, beta;
   unsigned int counter;
@@ -2964,31 +3166,33 @@ int build_cg_graph(pyib_ctx* ctx) {
   return PYIB_OK;
 }
 
-// PCG from warm start s with right-hand side residual res_e (ib_driver_np.py:311-410).
-int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
+// PCG from warm start s with right-hand side residual res_e (ib_driver_np.py:311-410),
+// in three parts so that a batch can run the iterations of many cases together:
+// solve_begin (tuning, state, k_cg_init; *iterate is false when the start already
+// meets the test), the iteration chunks (this context's CG graph, or a batched one),
+// and solve_end (true residual of the correction, s = x, statistics).
+int solve_begin(pyib_ctx* ctx, double dt, bool own_graph, bool* iterate) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
   RET(tune_matvec(ctx));
   if (ctx->use_fused) RET(tune_fused(ctx));
   RET(set_state_solver(ctx, dt, 1));
-  RET(build_cg_graph(ctx));
+  if (own_graph) RET(build_cg_graph(ctx));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   k_cg_init<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->res_e, ctx->s, prec, ctx->x, ctx->r,
                                                         ctx->p, ctx->partials, ctx->st);
   CKL();
   CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  const bool start_converged = ctx->st_host->eta < ctx->st_host->thresh;
+  *iterate = !(ctx->st_host->eta < ctx->st_host->thresh);
+  return PYIB_OK;
+}
+
+int solve_end(pyib_ctx* ctx, bool iterated, pyib_solve_stats* out) {
+  const long long ne = ctx->lay.nedge;
+  const double* prec = tp<double>(ctx, PYIB_T_PREC);
   int iters = 0;
-  if (!start_converged) {
-    const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
-    for (long long q = 0; q < max_chunks; ++q) {
-      CK(cudaGraphLaunch(ctx->cg_graph, ctx->stream));
-      ctx->launches += ctx->cg_graph_kernels;
-      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (ctx->st_host->done) break;
-    }
+  if (iterated) {
     if (!ctx->st_host->done) return set_err(ctx, PYIB_E_STATE, "CG loop did not terminate");
     iters = ctx->st_host->iters;
     // true residual of the correction x - s (ib_driver_np.py:404-410)
@@ -3034,6 +3238,26 @@ int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
                    "mixed_tolerance_ratio=%.6e",
                    iters, ctx->prm.cg_max, s.rel_residual, s.tol_ratio);
   return PYIB_OK;
+}
+
+// chunks of `check` iterations bounded by cg_max: the most a solve can replay
+long long max_cg_chunks(const pyib_ctx* ctx) {
+  return (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
+}
+
+int helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
+  bool iterate = false;
+  RET(solve_begin(ctx, dt, true, &iterate));
+  if (iterate) {
+    for (long long q = 0; q < max_cg_chunks(ctx); ++q) {
+      CK(cudaGraphLaunch(ctx->cg_graph, ctx->stream));
+      ctx->launches += ctx->cg_graph_kernels;
+      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (ctx->st_host->done) break;
+    }
+  }
+  return solve_end(ctx, iterate, out);
 }
 
 // ---- mixed precision --------------------------------------------------------
@@ -3151,9 +3375,14 @@ int clear_done(pyib_ctx* ctx) {
   return PYIB_OK;
 }
 
-// Mixed precision: the float64 stopping test of helm_solve on the float64 residual,
-// reached by one float32 PCG (Jacobi on diag(A)) with reliable float64 updates.
-int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
+// State of one mixed-precision solve between its parts (mixed_begin, the float32
+// iteration chunks, mixed_refine after each inner stop, mixed_end).
+struct MixRun {
+  double thresh = 0, l2_0 = 0, eta0 = 0, eta = 0, l2 = 0, eps2 = 0;
+  int inner_total = 0, sweeps = 0, max_sweeps = 40;
+};
+
+int mixed_begin(pyib_ctx* ctx, double dt, bool own_graph, MixRun& mr, bool* iterate) {
   const long long ne = ctx->lay.nedge;
   const double* prec = tp<double>(ctx, PYIB_T_PREC);
   RET(tune_matvec(ctx));
@@ -3169,81 +3398,111 @@ int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
     ctx->diag_for_rou = ctx->prm.rou;
   }
   RET(set_state_solver(ctx, dt, 1));
-  RET(build_mix_graph(ctx));
+  if (own_graph) RET(build_mix_graph(ctx));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   k_cg_init<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->res_e, ctx->s, prec, ctx->x, ctx->r,
                                                         ctx->p, ctx->partials, ctx->st);
   CKL();
   CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  const double thresh = ctx->st_host->thresh, l2_0 = ctx->st_host->l2_0, eta0 = ctx->st_host->eta;
-  double eta = eta0, l2 = l2_0;
-  int inner_total = 0, sweeps = 0;
-  const double eps2 = ctx->prm.mixed_tol * ctx->prm.mixed_tol;
-  const int max_sweeps = ctx->prm.mixed_max_sweeps > 0 ? ctx->prm.mixed_max_sweeps : 40;
+  mr = MixRun{};
+  mr.thresh = ctx->st_host->thresh;
+  mr.l2_0 = ctx->st_host->l2_0;
+  mr.eta0 = ctx->st_host->eta;
+  mr.eta = mr.eta0;
+  mr.l2 = mr.l2_0;
+  mr.eps2 = ctx->prm.mixed_tol * ctx->prm.mixed_tol;
+  mr.max_sweeps = ctx->prm.mixed_max_sweeps > 0 ? ctx->prm.mixed_max_sweeps : 40;
   // One float32 PCG (Jacobi on diag A) with reliable updates.  Whenever its residual
   // has dropped by mixed_tol since the last update, the float32 correction is folded
   // into x in float64 and r is recomputed in float64 (r -= A x32); the float32 CG then
   // continues from the new residual with the same search direction (no restart), and
   // the reference's float64 test on r decides when to stop.
+  k_mix_start<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
+                                                          ctx->p32, mr.eps2, ctx->partials, ctx->st);
+  CKL();
+  *iterate = !(mr.eta < mr.thresh) && mr.sweeps < mr.max_sweeps;
+  return PYIB_OK;
+}
+
+// After the float32 CG stopped (st_host read): x += x32, r -= A x32 in float64, the
+// reference's test on r; unless it holds, the float32 CG continues from the new
+// residual (*iterate stays true while sweeps remain).
+int mixed_refine(pyib_ctx* ctx, MixRun& mr, bool* iterate) {
+  const long long ne = ctx->lay.nedge;
+  const double* prec = tp<double>(ctx, PYIB_T_PREC);
   double* d = ctx->p;                 // float64 copy of the float32 correction
   double* q = ctx->w;                 // A d
-  k_mix_start<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
-                                                          ctx->p32, eps2, ctx->partials, ctx->st);
+  mr.inner_total += ctx->st_host->iters;
+  k_mix_widen<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, d, prec);
   CKL();
-  const long long max_chunks = (ctx->prm.cg_max + ctx->prm.check - 1) / ctx->prm.check + 1;
-  while (!(eta < thresh) && sweeps < max_sweeps) {
-    for (long long c = 0; c < max_chunks; ++c) {
-      CK(cudaGraphLaunch(ctx->mix_graph, ctx->stream));
-      ctx->launches += ctx->mix_graph_kernels;
-      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (ctx->st_host->done) break;
-    }
-    inner_total += ctx->st_host->iters;
-    // x += x32, r -= A x32 in float64
-    k_mix_widen<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->x32, d, prec);
-    CKL();
-    RET(clear_done(ctx));
-    RET(launch_matvec(ctx, d, q, 1, 0));
-    k_mix_fold<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, q, ctx->x, ctx->r, prec, ctx->partials,
-                                                           ctx->st);
-    CKL();
-    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    eta = ctx->st_host->true_eta;
-    l2 = ctx->st_host->true_l2;
-    ++sweeps;
-    if (!std::isfinite(eta) || eta < thresh) break;
-    k_mix_reliable<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
-                                                               eps2, ctx->partials, ctx->st);
-    CKL();
-    k_cg_p32<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r32, ctx->prec32, ctx->p32, ctx->st);
-    CKL();
+  RET(clear_done(ctx));
+  RET(launch_matvec(ctx, d, q, 1, 0));
+  k_mix_fold<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, d, q, ctx->x, ctx->r, prec, ctx->partials, ctx->st);
+  CKL();
+  CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  mr.eta = ctx->st_host->true_eta;
+  mr.l2 = ctx->st_host->true_l2;
+  ++mr.sweeps;
+  if (!std::isfinite(mr.eta) || mr.eta < mr.thresh) {
+    *iterate = false;
+    return PYIB_OK;
   }
+  k_mix_reliable<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r, ctx->prec32, ctx->r32, ctx->x32,
+                                                             mr.eps2, ctx->partials, ctx->st);
+  CKL();
+  k_cg_p32<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->r32, ctx->prec32, ctx->p32, ctx->st);
+  CKL();
+  *iterate = mr.sweeps < mr.max_sweeps;
+  return PYIB_OK;
+}
+
+int mixed_end(pyib_ctx* ctx, const MixRun& mr, pyib_solve_stats* out) {
+  const long long ne = ctx->lay.nedge;
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   CK(cudaMemcpyAsync(ctx->s, ctx->x, ne * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->cg_seconds += ms * 1e-3;
-  ctx->cg_iters += inner_total;
+  ctx->cg_iters += mr.inner_total;
+  const double eta = mr.eta, l2 = mr.l2, l2_0 = mr.l2_0, thresh = mr.thresh;
   const bool finite = std::isfinite(eta) && std::isfinite(l2) && eta >= 0 && l2 >= 0;
   pyib_solve_stats st{};
-  st.iterations = inner_total;
-  st.refinements = sweeps;
+  st.iterations = mr.inner_total;
+  st.refinements = mr.sweeps;
   st.rel_residual = finite && l2_0 > 0 ? std::sqrt(l2 / l2_0) : (finite && l2 == 0 ? 0.0 : INFINITY);
   st.tol_ratio = finite && thresh > 0 ? std::sqrt(eta / thresh) : (finite && eta == 0 ? 0.0 : INFINITY);
   st.converged = finite && eta <= thresh;
-  st.eta0 = eta0;
+  st.eta0 = mr.eta0;
   st.threshold = thresh;
   if (out) *out = st;
   if (ctx->prm.strict && !st.converged)
     return set_err(ctx, PYIB_E_NOCONV,
                    "mixed-precision Helmholtz solve did not converge: sweeps=%d, inner iterations=%d, "
                    "mixed_tolerance_ratio=%.6e",
-                   sweeps, inner_total, st.tol_ratio);
+                   mr.sweeps, mr.inner_total, st.tol_ratio);
   return PYIB_OK;
+}
+
+// Mixed precision: the float64 stopping test of helm_solve on the float64 residual,
+// reached by one float32 PCG (Jacobi on diag(A)) with reliable float64 updates.
+int helm_solve_mixed(pyib_ctx* ctx, double dt, pyib_solve_stats* out) {
+  MixRun mr;
+  bool iterate = false;
+  RET(mixed_begin(ctx, dt, true, mr, &iterate));
+  while (iterate) {
+    for (long long c = 0; c < max_cg_chunks(ctx); ++c) {
+      CK(cudaGraphLaunch(ctx->mix_graph, ctx->stream));
+      ctx->launches += ctx->mix_graph_kernels;
+      CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (ctx->st_host->done) break;
+    }
+    RET(mixed_refine(ctx, mr, &iterate));
+  }
+  return mixed_end(ctx, mr, out);
 }
 
 // ---- immersed boundary --------------------------------------------------
@@ -3389,24 +3648,40 @@ int ib_alloc(pyib_ctx* ctx, int M) {
 }
 
 // ---- one step ------------------------------------------------------------
-int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* markers,
-            const double* vel, pyib_step_stats* out) {
+// One time step (Driver.step, ib_driver_np.py:412-532) in parts, so that a batch can
+// run the Helmholtz solves of many cases together: step_begin (markers, held force,
+// calc_vel, the explicit convection/diffusion part, the guess), then for each inner
+// iteration step_rhs (force update of the direct mode, the residual, res_e), the
+// solve, and step_after_solve (statistics, calc_vel, the accumulated force update).
+struct StepRun {
+  double dt = 0.0, dt_old = 0.0;
+  int inner = 0, it = 0;
+  bool accumulated = false, ib = false;
+  pyib_step_stats st{};
+};
+
+int step_begin(pyib_ctx* ctx, StepRun& sr, double dt, double dt_old, int inner, const double* markers,
+               const double* vel) {
   if (!tables_ready(ctx) || !ctx->have_params) return set_err(ctx, PYIB_E_STATE, "context not ready");
-  const bool accumulated = ctx->prm.ib_mode == 0;
-  if (accumulated && inner < 2)
+  sr = StepRun{};
+  sr.dt = dt;
+  sr.dt_old = dt_old;
+  sr.inner = inner;
+  sr.it = 1;
+  sr.accumulated = ctx->prm.ib_mode == 0;
+  if (sr.accumulated && inner < 2)
     return set_err(ctx, PYIB_E_ARG, "accumulated_explicit requires at least 2 fluid inner iterations");
   if (inner < 1) return set_err(ctx, PYIB_E_ARG, "at least one fluid inner iteration");
   const pyib_params& P = ctx->prm;
-  const long long nc = ctx->lay.ncell, ne = ctx->lay.nedge;
-  const bool ib = ctx->M > 0;
-  pyib_step_stats st{};
-  st.all_converged = 1;
-  if (ib && markers) {
+  const long long ne = ctx->lay.nedge;
+  sr.ib = ctx->M > 0;
+  sr.st.all_converged = 1;
+  if (sr.ib && markers) {
     CK(cudaMemcpyAsync(ctx->mk, markers, 3 * ctx->M * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->mvel, vel, 3 * ctx->M * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     RET(ib_stencil(ctx));
-    if (accumulated) RET(ib_spread(ctx, ctx->fL, ctx->fE));   // held force follows the body (ib_driver_np.py:447-451)
-  } else if (ib && !ctx->stencil_valid) {
+    if (sr.accumulated) RET(ib_spread(ctx, ctx->fL, ctx->fE));   // held force follows the body (ib_driver_np.py:447-451)
+  } else if (sr.ib && !ctx->stencil_valid) {
     RET(ib_stencil(ctx));
   }
   RET(op_calc_vel(ctx));
@@ -3415,50 +3690,79 @@ int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* ma
   k_guess<<<grid_for(ne), kThreads, 0, ctx->stream>>>(ne, ctx->s, ctx->s_old, ctx->prev, dt, dt_old);
   CKL();
   RET(op_calc_vel(ctx));
-  for (int it = 1; it <= inner; ++it) {
-    if (ib && !accumulated) {
-      // direct mode: this iteration's force replaces the last (ib_driver_np.py:466-486)
-      RET(ib_interp(ctx, ctx->lag));
-      k_ib_force<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(ctx->M, ctx->mvel, ctx->lag, dt, ctx->dL);
-      CKL();
-      if (ctx->prm.ib_mode == 2) RET(ib_implicit_solve(ctx));
-      RET(ib_spread(ctx, ctx->dL, ctx->conv));   // conv is free scratch before op_convdiff
-      const double ra = rou * ctx->prm.ib_alpha;
-      k_set_scaled<<<grid_for(3 * nc), kThreads, 0, ctx->stream>>>(3 * nc, ctx->fE, ra, ctx->conv);
-      CKL();
-      k_set_scaled<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(3 * ctx->M, ctx->fL, ra, ctx->dL);
-      CKL();
-      st.ib_updates += 1;
-    }
-    RET(op_convdiff(ctx, 2, (ac * dt) * rou, ad * dt, dt, ctx->res_c0, ib ? ctx->fE : nullptr, ctx->res_c,
-                    nullptr));
-    RET(op_integr(ctx, ctx->res_c, nc, ctx->F));
-    RET(op_rot(ctx, ctx->F, ctx->res_e));
-    pyib_solve_stats ss{};
-    int rc = ctx->prm.precision == 1 ? helm_solve_mixed(ctx, dt, &ss) : helm_solve(ctx, dt, &ss);
-    st.max_iterations = ss.iterations > st.max_iterations ? ss.iterations : st.max_iterations;
-    st.total_iterations += ss.iterations;
-    st.max_rel_residual = fmax(st.max_rel_residual, ss.rel_residual);
-    st.max_tol_ratio = fmax(st.max_tol_ratio, ss.tol_ratio);
-    st.all_converged = st.all_converged && ss.converged;
-    if (out) *out = st;
-    if (rc != PYIB_OK) return rc;
-    RET(op_calc_vel(ctx));
-    if (ib && accumulated && it == 1) {
-      RET(ib_interp(ctx, ctx->lag));
-      k_ib_force<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(ctx->M, ctx->mvel, ctx->lag, dt, ctx->dL);
-      CKL();
-      RET(ib_spread(ctx, ctx->dL, ctx->conv));   // conv is free scratch here
-      k_axpy_scaled<<<grid_for(3 * nc), kThreads, 0, ctx->stream>>>(3 * nc, ctx->fE, rou, ctx->conv);
-      CKL();
-      k_axpy_scaled<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(3 * ctx->M, ctx->fL, rou, ctx->dL);
-      CKL();
-      st.ib_updates += 1;
-    }
-  }
-  RET(check_dev_err(ctx));
-  if (out) *out = st;
   return PYIB_OK;
+}
+
+int step_rhs(pyib_ctx* ctx, StepRun& sr) {
+  const pyib_params& P = ctx->prm;
+  const long long nc = ctx->lay.ncell;
+  const double dt = sr.dt, rou = P.rou, ac = P.ac, ad = P.ad;
+  if (sr.ib && !sr.accumulated) {
+    // direct mode: this iteration's force replaces the last (ib_driver_np.py:466-486)
+    RET(ib_interp(ctx, ctx->lag));
+    k_ib_force<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(ctx->M, ctx->mvel, ctx->lag, dt, ctx->dL);
+    CKL();
+    if (ctx->prm.ib_mode == 2) RET(ib_implicit_solve(ctx));
+    RET(ib_spread(ctx, ctx->dL, ctx->conv));   // conv is free scratch before op_convdiff
+    const double ra = rou * ctx->prm.ib_alpha;
+    k_set_scaled<<<grid_for(3 * nc), kThreads, 0, ctx->stream>>>(3 * nc, ctx->fE, ra, ctx->conv);
+    CKL();
+    k_set_scaled<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(3 * ctx->M, ctx->fL, ra, ctx->dL);
+    CKL();
+    sr.st.ib_updates += 1;
+  }
+  RET(op_convdiff(ctx, 2, (ac * dt) * rou, ad * dt, dt, ctx->res_c0, sr.ib ? ctx->fE : nullptr, ctx->res_c,
+                  nullptr));
+  RET(op_integr(ctx, ctx->res_c, nc, ctx->F));
+  RET(op_rot(ctx, ctx->F, ctx->res_e));
+  return PYIB_OK;
+}
+
+// statistics of this iteration's solve (kept when the solve failed), then the rest of
+// the inner iteration; sr.it moves to the next one
+int step_after_solve(pyib_ctx* ctx, StepRun& sr, const pyib_solve_stats& ss, int solve_rc, pyib_step_stats* out) {
+  const long long nc = ctx->lay.ncell;
+  const double rou = ctx->prm.rou;
+  sr.st.max_iterations = ss.iterations > sr.st.max_iterations ? ss.iterations : sr.st.max_iterations;
+  sr.st.total_iterations += ss.iterations;
+  sr.st.max_rel_residual = fmax(sr.st.max_rel_residual, ss.rel_residual);
+  sr.st.max_tol_ratio = fmax(sr.st.max_tol_ratio, ss.tol_ratio);
+  sr.st.all_converged = sr.st.all_converged && ss.converged;
+  if (out) *out = sr.st;
+  if (solve_rc != PYIB_OK) return solve_rc;
+  RET(op_calc_vel(ctx));
+  if (sr.ib && sr.accumulated && sr.it == 1) {
+    RET(ib_interp(ctx, ctx->lag));
+    k_ib_force<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(ctx->M, ctx->mvel, ctx->lag, sr.dt, ctx->dL);
+    CKL();
+    RET(ib_spread(ctx, ctx->dL, ctx->conv));   // conv is free scratch here
+    k_axpy_scaled<<<grid_for(3 * nc), kThreads, 0, ctx->stream>>>(3 * nc, ctx->fE, rou, ctx->conv);
+    CKL();
+    k_axpy_scaled<<<grid_for(3 * ctx->M), kThreads, 0, ctx->stream>>>(3 * ctx->M, ctx->fL, rou, ctx->dL);
+    CKL();
+    sr.st.ib_updates += 1;
+  }
+  ++sr.it;
+  return PYIB_OK;
+}
+
+int step_end(pyib_ctx* ctx, StepRun& sr, pyib_step_stats* out) {
+  RET(check_dev_err(ctx));
+  if (out) *out = sr.st;
+  return PYIB_OK;
+}
+
+int do_step(pyib_ctx* ctx, double dt, double dt_old, int inner, const double* markers, const double* vel,
+            pyib_step_stats* out) {
+  StepRun sr;
+  RET(step_begin(ctx, sr, dt, dt_old, inner, markers, vel));
+  while (sr.it <= sr.inner) {
+    RET(step_rhs(ctx, sr));
+    pyib_solve_stats ss{};
+    const int rc = ctx->prm.precision == 1 ? helm_solve_mixed(ctx, dt, &ss) : helm_solve(ctx, dt, &ss);
+    RET(step_after_solve(ctx, sr, ss, rc, out));
+  }
+  return step_end(ctx, sr, out);
 }
 
 }  // namespace
@@ -3575,6 +3879,310 @@ static int graph_cg(pyib_ctx* ctx, long long n, const long long* ptr, const int*
     if (!std::isfinite(h.rr)) return set_err(ctx, PYIB_E_NONFINITE, "graph PCG: non-finite residual");
   }
   CK(cudaEventRecord(ctx->ev1, st));
+  return PYIB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: independent cases on one GPU whose CG iterations run together, one launch
+// per kernel stage over the tiles of every case still iterating (k_b* kernels),
+// `check` iterations to a CUDA graph.  Everything else of a step runs per case on the
+// case's own stream, through the same step parts as pyib_step.
+// ---------------------------------------------------------------------------
+struct pyib_batch {
+  std::vector<pyib_ctx*> cs;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  BCase* d_cases = nullptr;        // one per case, in the precision of the current solve
+  int2* d_blk = nullptr;           // (case, block within the case's grid) of every block of every stage
+  size_t blk_cap = 0;              // int2 entries d_blk holds
+  std::vector<BCase> h_cases;
+  std::vector<int2> h_blk;
+  // stage q of group g: h_blk[blk_off[g][q] .. blk_off[g][q+1])
+  long long blk_off[kBatchGroups][kBStages + 1] = {};
+  cudaStream_t gstream[kBatchGroups] = {};     // capture branches of the groups
+  cudaEvent_t fork = nullptr, join[kBatchGroups] = {};
+  cudaGraphExec_t graph = nullptr;
+  std::vector<char> graph_for;     // the iterating cases the graph was captured for
+  int graph_prec = -1;
+  long long graph_kernels = 0;     // kernel nodes of one replay
+  long long launches = 0;          // batched kernels launched (replays x kernel nodes)
+  long long captures = 0;          // graph captures
+  double chunk_seconds = 0.0;      // CUDA-event time of the batched chunks
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static int batch_err(pyib_batch* b, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  b->err = buf;
+  return code;
+}
+
+#define BCK(call)                                                                      \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return batch_err(b, PYIB_E_CUDA, "%s failed: %s (%s:%d)", #call,                 \
+                       cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+  } while (0)
+
+// a failing case's status, with its message as the batch's
+static int batch_case_rc(pyib_batch* b, int c, int rc) {
+  if (rc != PYIB_OK) b->err = "case " + std::to_string(c) + ": " + b->cs[c]->err;
+  return rc;
+}
+
+// the device view of case c for a solve in float64 (prec 0) or float32 (prec 1)
+static BCase batch_view(pyib_ctx* ctx, int prec) {
+  BCase q{};
+  q.m = prec ? ctx->meta32 : ctx->meta;
+  q.st = ctx->st;
+  q.partials = ctx->partials;
+  if (prec) {
+    q.p = ctx->p32; q.w = ctx->w32; q.vcm = ctx->vcm32; q.vq = ctx->vq32; q.r = ctx->r32; q.x = ctx->x32;
+    q.pa_val = ctx->pa_val32; q.pv_val = ctx->pv_val32; q.pr_val = ctx->pr_val32;
+  } else {
+    q.p = ctx->p; q.w = ctx->w; q.vcm = ctx->vcm; q.vq = ctx->vq; q.r = ctx->r; q.x = ctx->x;
+    q.pa_val = tp<double>(ctx, PYIB_T_PA_VAL); q.pv_val = tp<double>(ctx, PYIB_T_PV_VAL);
+    q.pr_val = tp<double>(ctx, PYIB_T_PR_VAL);
+  }
+  q.pa_ids = tp<int>(ctx, PYIB_T_PA_IDS); q.pa_col = tp<int>(ctx, PYIB_T_PA_COL);
+  q.pv_ids = tp<int>(ctx, PYIB_T_PV_IDS); q.pv_col = tp<int>(ctx, PYIB_T_PV_COL);
+  q.pr_ids = tp<int>(ctx, PYIB_T_PR_IDS); q.pr_col = tp<int>(ctx, PYIB_T_PR_COL);
+  q.pa_ptr = tp<long long>(ctx, PYIB_T_PA_PTR); q.pv_ptr = tp<long long>(ctx, PYIB_T_PV_PTR);
+  q.pr_ptr = tp<long long>(ctx, PYIB_T_PR_PTR);
+  q.prec_bits = tp<unsigned int>(ctx, PYIB_T_PREC_BITS);
+  q.pr_bits = tp<unsigned int>(ctx, PYIB_T_PR_BITS);
+  q.prec = tp<double>(ctx, PYIB_T_PREC);
+  q.dinv = ctx->prec32;
+  q.nA = ctx->nA; q.nV = ctx->nV; q.nR = ctx->nR;
+  q.ne = ctx->lay.nedge; q.nc = ctx->lay.ncell;
+  // Deep z-chunks for the batched tiles: a batched block first looks up its case, so
+  // longer blocks amortise that.  The cell kernels compute cell by cell and the dot's
+  // partials are indexed by plane, so the depths change no result.
+  set_grids(q.m, kBatchCellDepth, kBatchNodeDepth);
+  const Meta& m = q.m;
+  q.nblk[0] = m.gxA * m.gyA * m.gzA;
+  q.nblk[1] = q.nA > 0 ? patch_grid(3 * q.nA) : 0;
+  q.nblk[2] = m.gxV * m.gyA * m.gzA;
+  q.nblk[3] = q.nV > 0 ? patch_grid(q.nV) : 0;
+  q.nblk[4] = m.gxR * m.gyR * m.gzR;
+  q.nblk[5] = patch_grid(q.nR);        // also the final reduction of p.w
+  q.nblk[6] = grid_for(q.ne);
+  q.nblk[7] = grid_for(q.ne);
+  return q;
+}
+
+// The iterating cases in kBatchGroups groups of about equal work (edges; largest
+// first, each to the lightest group), and the block table of every stage of every
+// group: the blocks of each case's own grids, so every reduction sums in the case's
+// own order.
+static int batch_blocks(pyib_batch* b, const std::vector<char>& on) {
+  const int n = (int)b->cs.size();
+  std::vector<int> order;
+  for (int c = 0; c < n; ++c)
+    if (on[c]) order.push_back(c);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return b->h_cases[x].ne > b->h_cases[y].ne; });
+  std::vector<int> group(n, -1);
+  long long load[kBatchGroups] = {0};
+  for (int c : order) {
+    int g = 0;
+    for (int k = 1; k < kBatchGroups; ++k)
+      if (load[k] < load[g]) g = k;
+    group[c] = g;
+    load[g] += b->h_cases[c].ne;
+  }
+  b->h_blk.clear();
+  for (int g = 0; g < kBatchGroups; ++g) {
+    for (int q = 0; q < kBStages; ++q) {
+      b->blk_off[g][q] = (long long)b->h_blk.size();
+      for (int c = 0; c < n; ++c)
+        if (group[c] == g)
+          for (int k = 0; k < b->h_cases[c].nblk[q]; ++k) b->h_blk.push_back(make_int2(c, k));
+    }
+    b->blk_off[g][kBStages] = (long long)b->h_blk.size();
+  }
+  if (b->h_blk.size() > b->blk_cap) {
+    if (b->d_blk) BCK(cudaFree(b->d_blk));
+    b->d_blk = nullptr;
+    b->blk_cap = 0;
+    BCK(cudaMalloc((void**)&b->d_blk, b->h_blk.size() * sizeof(int2)));
+    b->blk_cap = b->h_blk.size();
+  }
+  if (!b->h_blk.empty())
+    BCK(cudaMemcpyAsync(b->d_blk, b->h_blk.data(), b->h_blk.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                        b->stream));
+  return PYIB_OK;
+}
+
+// (Re)captures the chunk graph: `check` iterations of the 8 stages over the cases in on.
+static int batch_graph(pyib_batch* b, int prec, const std::vector<char>& on) {
+  if (b->graph && b->graph_prec == prec && b->graph_for == on) return PYIB_OK;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  RET(batch_blocks(b, on));
+  BCK(cudaStreamSynchronize(b->stream));   // the block table is in place before any branch reads it
+  const int check = b->cs[0]->prm.check;
+  cudaGraph_t g;
+  BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  const dim3 blk2(TX, TY, 1);
+  // errors inside the capture are kept until it has ended, so the stream never stays capturing
+  cudaError_t ce = cudaEventRecord(b->fork, b->stream);
+  for (int grp = 0; grp < kBatchGroups; ++grp) {
+   if (b->blk_off[grp][kBStages] == b->blk_off[grp][0]) continue;
+   cudaStream_t gs = b->gstream[grp];
+   if (ce == cudaSuccess) ce = cudaStreamWaitEvent(gs, b->fork, 0);
+   for (int it = 0; it < check; ++it) {
+    for (int q = 0; q < kBStages; ++q) {
+      const int total = (int)(b->blk_off[grp][q + 1] - b->blk_off[grp][q]);
+      if (total == 0) continue;
+      const int2* st = b->d_blk + b->blk_off[grp][q];
+      if (prec) {
+        switch (q) {
+          case 0: k_bA<float><<<total, blk2, 0, gs>>>(b->d_cases, st); break;
+          case 1: k_bpatchA<float><<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          case 2: k_bV<float><<<total, blk2, 0, gs>>>(b->d_cases, st); break;
+          case 3: k_bpatchV<float><<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          case 4: k_bRI<float><<<total, blk2, 0, gs>>>(b->d_cases, st); break;
+          case 5: k_bpatchRI<float><<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          case 6: k_bupdate32<<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          default: k_bdir32<<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+        }
+      } else {
+        switch (q) {
+          case 0: k_bA<double><<<total, blk2, 0, gs>>>(b->d_cases, st); break;
+          case 1: k_bpatchA<double><<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          case 2: k_bV<double><<<total, blk2, 0, gs>>>(b->d_cases, st); break;
+          case 3: k_bpatchV<double><<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          case 4: k_bRI<double><<<total, blk2, 0, gs>>>(b->d_cases, st); break;
+          case 5: k_bpatchRI<double><<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          case 6: k_bupdate<<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+          default: k_bdir<<<total, kThreads, 0, gs>>>(b->d_cases, st); break;
+        }
+      }
+    }
+   }
+   if (ce == cudaSuccess) ce = cudaEventRecord(b->join[grp], gs);
+   if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[grp], 0);
+  }
+  const cudaError_t le = cudaGetLastError();
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (ce != cudaSuccess || e != cudaSuccess) {
+    if (e == cudaSuccess) cudaGraphDestroy(g);
+    return batch_err(b, PYIB_E_CUDA, "batch graph capture failed: %s",
+                     cudaGetErrorString(ce != cudaSuccess ? ce : e));
+  }
+  if (le != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return batch_err(b, PYIB_E_CUDA, "batched launch failed: %s", cudaGetErrorString(le));
+  }
+  b->graph_kernels = graph_kernels(g);
+  const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return batch_err(b, PYIB_E_CUDA, "batch graph instantiate failed: %s", cudaGetErrorString(ie));
+  b->graph_prec = prec;
+  b->graph_for = on;
+  ++b->captures;
+  return PYIB_OK;
+}
+
+// Replays the chunk graph over the cases in on, then reads every iterating case's
+// state (one copy each, one synchronisation).
+static int batch_chunk(pyib_batch* b, int prec, const std::vector<char>& on) {
+  RET(batch_graph(b, prec, on));
+  BCK(cudaEventRecord(b->ev0, b->stream));
+  BCK(cudaGraphLaunch(b->graph, b->stream));
+  BCK(cudaEventRecord(b->ev1, b->stream));
+  b->launches += b->graph_kernels;
+  for (size_t c = 0; c < b->cs.size(); ++c)
+    if (on[c])
+      BCK(cudaMemcpyAsync(b->cs[c]->st_host, b->cs[c]->st, sizeof(CGState), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  float ms = 0.f;
+  BCK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  b->chunk_seconds += ms * 1e-3;
+  return PYIB_OK;
+}
+
+// One Helmholtz solve of every case (helm_solve or helm_solve_mixed), the CG
+// iterations of all cases batched.  rc[c] is case c's status; the batch's own
+// failures (CUDA errors of the batched launches) are returned.
+static int batch_solve(pyib_batch* b, const std::vector<double>& dt, std::vector<pyib_solve_stats>& ss,
+                       std::vector<int>& rc) {
+  const int n = (int)b->cs.size();
+  const int prec = b->cs[0]->prm.precision == 1 ? 1 : 0;
+  std::vector<char> on(n, 0);
+  std::vector<MixRun> mr(n);
+  std::vector<long long> chunks(n, 0);
+  std::vector<char> iterated(n, 0);
+  for (int c = 0; c < n; ++c) {
+    pyib_ctx* ctx = b->cs[c];
+    if (rc[c] != PYIB_OK) continue;
+    bool it = false;
+    rc[c] = prec ? mixed_begin(ctx, dt[c], false, mr[c], &it) : solve_begin(ctx, dt[c], false, &it);
+    if (rc[c] == PYIB_OK) BCK(cudaStreamSynchronize(ctx->stream));   // its start is in place before the chunks
+    on[c] = rc[c] == PYIB_OK && it;
+    iterated[c] = on[c];
+    b->h_cases[c] = batch_view(ctx, prec);
+  }
+  BCK(cudaMemcpyAsync(b->d_cases, b->h_cases.data(), n * sizeof(BCase), cudaMemcpyHostToDevice, b->stream));
+  for (;;) {
+    bool any = false;
+    for (int c = 0; c < n; ++c) any = any || on[c];
+    if (!any) break;
+    RET(batch_chunk(b, prec, on));
+    for (int c = 0; c < n; ++c) {
+      if (!on[c]) continue;
+      pyib_ctx* ctx = b->cs[c];
+      ++chunks[c];
+      if (!ctx->st_host->done && chunks[c] < max_cg_chunks(ctx)) continue;
+      if (prec) {
+        // the float32 CG stopped: fold its correction into x and decide
+        bool more = false;
+        rc[c] = mixed_refine(ctx, mr[c], &more);
+        if (rc[c] == PYIB_OK) BCK(cudaStreamSynchronize(ctx->stream));
+        on[c] = rc[c] == PYIB_OK && more;
+        chunks[c] = 0;
+      } else {
+        on[c] = 0;
+      }
+    }
+  }
+  for (int c = 0; c < n; ++c) {
+    if (rc[c] != PYIB_OK) continue;
+    pyib_ctx* ctx = b->cs[c];
+    rc[c] = prec ? mixed_end(ctx, mr[c], &ss[c]) : solve_end(ctx, iterated[c] != 0, &ss[c]);
+  }
+  return PYIB_OK;
+}
+
+// One time step of every case (do_step), the Helmholtz solves batched.
+static int batch_step(pyib_batch* b, const double* dt, const double* dt_old, int inner,
+                      const double* const* markers, const double* const* vel, pyib_step_stats* stats) {
+  const int n = (int)b->cs.size();
+  std::vector<StepRun> sr(n);
+  std::vector<int> rc(n, PYIB_OK);
+  std::vector<double> dts(dt, dt + n);
+  for (int c = 0; c < n; ++c) {
+    pyib_ctx* ctx = b->cs[c];
+    RET(batch_case_rc(b, c, step_begin(ctx, sr[c], dt[c], dt_old[c], inner, markers ? markers[c] : nullptr,
+                                       vel ? vel[c] : nullptr)));
+  }
+  for (int it = 1; it <= inner; ++it) {
+    for (int c = 0; c < n; ++c) RET(batch_case_rc(b, c, step_rhs(b->cs[c], sr[c])));
+    std::vector<pyib_solve_stats> ss(n);
+    RET(batch_solve(b, dts, ss, rc));
+    for (int c = 0; c < n; ++c)
+      RET(batch_case_rc(b, c, step_after_solve(b->cs[c], sr[c], ss[c], rc[c], stats ? &stats[c] : nullptr)));
+  }
+  for (int c = 0; c < n; ++c) RET(batch_case_rc(b, c, step_end(b->cs[c], sr[c], stats ? &stats[c] : nullptr)));
   return PYIB_OK;
 }
 
@@ -3930,6 +4538,99 @@ int pyib_step(pyib_ctx* ctx, double dt, double dt_old, int32_t inner, const doub
   if ((markers == nullptr) != (vel == nullptr)) return set_err(ctx, PYIB_E_ARG, "markers and vel go together");
   CK(cudaSetDevice(ctx->device));
   return do_step(ctx, dt, dt_old, inner, markers, vel, stats);
+}
+
+int pyib_batch_create(pyib_ctx* const* ctxs, int32_t n, pyib_batch** out) {
+  if (!ctxs || n < 1 || !out) return PYIB_E_ARG;
+  *out = nullptr;
+  for (int c = 0; c < n; ++c) {
+    if (!ctxs[c]) return PYIB_E_ARG;
+    if (ctxs[c]->device != ctxs[0]->device) return set_err(ctxs[c], PYIB_E_ARG, "a batch lives on one device");
+    for (int d = 0; d < c; ++d)
+      if (ctxs[d] == ctxs[c]) return set_err(ctxs[c], PYIB_E_ARG, "a context appears twice in the batch");
+  }
+  pyib_batch* b = new pyib_batch();
+  b->cs.assign(ctxs, ctxs + n);
+  b->device = ctxs[0]->device;
+  b->h_cases.assign(n, BCase{});
+  auto fail = [&](cudaError_t e) {
+    const std::string msg = cudaGetErrorString(e);
+    pyib_batch_destroy(b);
+    return set_err(ctxs[0], PYIB_E_CUDA, "batch setup failed: %s", msg.c_str());
+  };
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_cases, n * sizeof(BCase));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (int g = 0; g < kBatchGroups && e == cudaSuccess; ++g) {
+    e = cudaStreamCreateWithFlags(&b->gstream[g], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[g], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) return fail(e);
+  *out = b;
+  return PYIB_OK;
+}
+
+int pyib_batch_destroy(pyib_batch* b) {
+  if (!b) return PYIB_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->d_cases) cudaFree(b->d_cases);
+  if (b->d_blk) cudaFree(b->d_blk);
+  for (int g = 0; g < kBatchGroups; ++g) {
+    if (b->join[g]) cudaEventDestroy(b->join[g]);
+    if (b->gstream[g]) cudaStreamDestroy(b->gstream[g]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return PYIB_OK;
+}
+
+int pyib_batch_last_error(const pyib_batch* b, char* buf, size_t n) {
+  if (!b || !buf || n == 0) return PYIB_E_ARG;
+  snprintf(buf, n, "%s", b->err.c_str());
+  return PYIB_OK;
+}
+
+int pyib_batch_step(pyib_batch* b, const double* dt, const double* dt_old, int32_t inner,
+                    const double* const* markers, const double* const* vel, pyib_step_stats* stats) {
+  if (!b || !dt || !dt_old) return PYIB_E_ARG;
+  b->err.clear();
+  const int n = (int)b->cs.size();
+  if ((markers == nullptr) != (vel == nullptr)) return batch_err(b, PYIB_E_ARG, "markers and vel go together");
+  for (int c = 0; c < n; ++c) {
+    const pyib_ctx* ctx = b->cs[c];
+    if (!(dt[c] > 0) || !(dt_old[c] > 0)) return batch_err(b, PYIB_E_ARG, "case %d: dt must be positive", c);
+    if (markers && ((markers[c] == nullptr) != (vel[c] == nullptr)))
+      return batch_err(b, PYIB_E_ARG, "case %d: markers and vel go together", c);
+    if (!ctx->have_params) return batch_err(b, PYIB_E_STATE, "case %d: context not ready", c);
+    if (ctx->prm.precision != b->cs[0]->prm.precision)
+      return batch_err(b, PYIB_E_ARG, "the cases of a batch share one precision");
+    if (ctx->prm.check != b->cs[0]->prm.check)
+      return batch_err(b, PYIB_E_ARG, "the cases of a batch share one CG check interval");
+    if (ctx->use_fused) return batch_err(b, PYIB_E_ARG, "case %d: the single-pass matvec is not batched", c);
+  }
+  BCK(cudaSetDevice(b->device));
+  return batch_step(b, dt, dt_old, inner, markers, vel, stats);
+}
+
+int pyib_batch_timing(pyib_batch* b, double* out, int32_t reset) {
+  if (!b || !out) return PYIB_E_ARG;
+  out[0] = b->chunk_seconds;
+  out[1] = (double)b->launches;
+  out[2] = (double)b->captures;
+  if (reset) {
+    b->chunk_seconds = 0.0;
+    b->launches = 0;
+    b->captures = 0;
+  }
+  return PYIB_OK;
 }
 
 int pyib_ib_stencil(pyib_ctx* ctx) {

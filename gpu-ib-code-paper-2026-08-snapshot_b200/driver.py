@@ -169,7 +169,16 @@ class B200Driver:
 
     def step(self, s, s_old, dt, dt_old, inner=4):
         """One fluid step, ib_driver_np.py:412-532."""
-        sv = self.solver
+        mk, vel = self._step_inputs(s, s_old, dt)
+        st = _lib.StepStats()
+        try:
+            self.solver.h.call("pyib_step", C.c_double(dt), C.c_double(dt_old), int(inner), mk, vel, C.byref(st))
+        finally:
+            self._step_stats(st)
+        return self._step_outputs(dt)
+
+    # the parts of step around the library call (shared with step_batch)
+    def _step_inputs(self, s, s_old, dt):
         self._put_edges("S", s)
         self._put_edges("S_OLD", s_old)
         self._step_count += 1
@@ -181,17 +190,19 @@ class B200Driver:
             self._vel = np.ascontiguousarray(v, dtype=np.float64)
             mk = self._markers.ctypes.data_as(C.c_void_p)
             vel = self._vel.ctypes.data_as(C.c_void_p)
-        st = _lib.StepStats()
-        try:
-            sv.h.call("pyib_step", C.c_double(dt), C.c_double(dt_old), int(inner), mk, vel, C.byref(st))
-        finally:
-            self.helmholtz_iterations_last_step = int(st.max_iterations)
-            self.helmholtz_total_iterations_last_step = int(st.total_iterations)
-            self.helmholtz_relative_residual_last_step = float(st.max_rel_residual)
-            self.helmholtz_tolerance_ratio_last_step = float(st.max_tol_ratio)
-            self.helmholtz_converged_last_step = bool(st.all_converged)
-            self.ib_force_updates_last_step = int(st.ib_updates)
-            self.ib_force_update_count += int(st.ib_updates)
+        return mk, vel
+
+    def _step_stats(self, st):
+        self.helmholtz_iterations_last_step = int(st.max_iterations)
+        self.helmholtz_total_iterations_last_step = int(st.total_iterations)
+        self.helmholtz_relative_residual_last_step = float(st.max_rel_residual)
+        self.helmholtz_tolerance_ratio_last_step = float(st.max_tol_ratio)
+        self.helmholtz_converged_last_step = bool(st.all_converged)
+        self.ib_force_updates_last_step = int(st.ib_updates)
+        self.ib_force_update_count += int(st.ib_updates)
+
+    def _step_outputs(self, dt):
+        sv = self.solver
         self.last_step_dt = float(dt)
         self.last_helm_m = self.helmholtz_iterations_last_step
         return (DeviceField(sv, "S"), DeviceField(sv, "VC", (3, sv.lay.NC + sv.bfaces.size)),
@@ -269,3 +280,30 @@ class B200Driver:
         if not hasattr(self, "_maps"):
             self._desc, self._maps = self.layout.export_mesh()
         return self._desc, self._maps
+
+
+def step_batch(batch, drivers, states, dts, dt_olds, inner=4):
+    """``Driver.step`` of several drivers at once through one ``pyib_batch`` (built
+    over the drivers' contexts, in this order): ``states`` holds each driver's
+    ``(s, s_old)``; returns each driver's ``(s, vc, s_old)`` as ``step`` does.  The
+    Helmholtz solves of all drivers run as batched CG iterations; every driver ends
+    in the state its own ``step`` would give."""
+    n = len(drivers)
+    mks = (C.c_void_p * n)()
+    vels = (C.c_void_p * n)()
+    use_markers = False
+    for q, (drv, (s, s_old), dt) in enumerate(zip(drivers, states, dts)):
+        mk, vel = drv._step_inputs(s, s_old, dt)
+        if mk is not None:
+            use_markers = True
+            mks[q], vels[q] = mk.value, vel.value
+    stats = (_lib.StepStats * n)()
+    dt_a = (C.c_double * n)(*[float(x) for x in dts])
+    dto_a = (C.c_double * n)(*[float(x) for x in dt_olds])
+    try:
+        batch.call("pyib_batch_step", dt_a, dto_a, int(inner), mks if use_markers else None,
+                   vels if use_markers else None, stats)
+    finally:
+        for drv, st in zip(drivers, stats):
+            drv._step_stats(st)
+    return [drv._step_outputs(dt) for drv, dt in zip(drivers, dts)]

@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 
 from .cases import R, SphereCase
-from .driver import B200Driver
+from .driver import B200Driver, step_batch
 
 
 class SphereLoads:
@@ -115,3 +115,22 @@ class SphereRun:
         load = self.loads.advance(self.centre(self.drv.time), self.dt)
         self.step_index = k
         return load
+
+
+def advance_batch(batch, runs, inner=4):
+    """``SphereRun.advance`` of several runs at once: one step of every run through the
+    ``pyib_batch`` ``batch`` (built over the runs' contexts, in this order), the
+    Helmholtz solves batched; returns each run's load.  Each run ends in the state
+    its own ``advance`` would give."""
+    for r in runs:
+        r.drv.time = r.step_index * r.dt
+    out = step_batch(batch, [r.drv for r in runs], [(r.s, r.s_old) for r in runs], [r.dt for r in runs],
+                     [r.dt for r in runs], inner=inner)
+    loads = []
+    for r, (s, vc, s_old) in zip(runs, out):
+        k = r.step_index + 1
+        r.s, r.vc, r.s_old = s, vc, s_old
+        r.drv.time = k * r.dt
+        loads.append(r.loads.advance(r.centre(r.drv.time), r.dt))
+        r.step_index = k
+    return loads

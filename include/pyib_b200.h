@@ -201,6 +201,31 @@ int pyib_helm_solve(pyib_ctx* ctx, double dt, pyib_solve_stats* stats);
 int pyib_step(pyib_ctx* ctx, double dt, double dt_old, int32_t inner,
               const double* markers, const double* vel, pyib_step_stats* stats);
 
+/* ---- batches of independent cases on one GPU ------------------------------- */
+/* No counterpart in the reference, which runs one case per process
+ * (ib_case.py:1413-1648).  A batch steps many cases of uneven size together: each
+ * step runs pyib_step's parts per case, and the CG iterations of every case's
+ * Helmholtz solves run together, one launch per kernel stage (curl+interp, viscous
+ * and integr+rot templates with their exact rows, residual update, direction
+ * update) over the tiles of all cases still iterating, `check` iterations to one
+ * CUDA graph.  Each case computes exactly what pyib_step computes on its own
+ * context (same kernels, grids and reduction orders).  The contexts stay owned by
+ * the caller, share one device, one precision and one CG check interval, and must
+ * not be used from another thread while a batch call runs. */
+typedef struct pyib_batch pyib_batch;
+int pyib_batch_create(pyib_ctx* const* ctxs, int32_t n, pyib_batch** out);
+int pyib_batch_destroy(pyib_batch* batch);
+int pyib_batch_last_error(const pyib_batch* batch, char* buf, size_t n);
+/* One step of every case: dt[c], dt_old[c] and (when markers is not NULL) the
+ * prescribed marker positions and velocities of case c, as pyib_step; stats[c]
+ * receives case c's statistics.  A failing case stops the call with its status and
+ * its message (pyib_batch_last_error). */
+int pyib_batch_step(pyib_batch* batch, const double* dt, const double* dt_old, int32_t inner,
+                    const double* const* markers, const double* const* vel, pyib_step_stats* stats);
+/* out[0] CUDA-event seconds of the batched iteration chunks, out[1] batched kernels
+ * launched, out[2] graph captures (out holds 3 doubles); reset clears them. */
+int pyib_batch_timing(pyib_batch* batch, double* out, int32_t reset);
+
 /* ---- immersed boundary (ib_immersed.py) ------------------------------------ */
 /* 5^3 stencil ids and weights (ImmersedBoundary._build_cells_weights, 63-81). */
 int pyib_ib_stencil(pyib_ctx* ctx);

@@ -32,3 +32,31 @@ def test_concurrent_equals_sequential():
         assert a.loads.latest["body_force"].tolist() == b.loads.latest["body_force"].tolist()
     con.close()
     seq.close()
+
+
+def _per_case(run):
+    return [(np.asarray(r.s).copy(), np.asarray(r.drv.ib_force_L).copy(), r.loads.latest["body_force"].tolist(),
+             r.drv.helmholtz_total_iterations_last_step) for r in run.runs]
+
+
+@pytest.mark.parametrize("precision", ["float64", "mixed"])
+def test_batched_equals_sequential(precision):
+    """One pyib_batch over all cases (the CG iterations of every case as one launch per
+    kernel stage) gives every case the bits of its own steps, in both precisions."""
+    bat = BatchRun(_cases(), precision=precision)
+    seq = BatchRun(_cases(), precision=precision)
+    bat.tune()
+    seq.tune()
+    for _ in range(2):
+        _, s1 = bat.advance(1, batched=True)
+        _, s2 = seq.advance(1, concurrent=False)
+        assert s1 == s2
+        for a, b in zip(_per_case(bat), _per_case(seq)):
+            assert np.array_equal(a[0], b[0])
+            assert np.array_equal(a[1], b[1])
+            assert a[2] == b[2]
+            assert a[3] == b[3]
+    t = bat.batch_timing()
+    assert t["batched_launches"] > 0 and t["chunk_seconds"] > 0 and t["graph_captures"] >= 1
+    bat.close()
+    seq.close()
