@@ -812,9 +812,11 @@ def run_batch(args, world, rank, local):
     graph-captured), concurrently (one host thread and stream per case) and one
     case at a time.
 
-    Each timing advances every case by ``--steps`` steps (consecutive steps of the
-    same runs: batched, then concurrently, then sequentially); host wall clock
-    around each phase, every case's last call having waited for its own stream.
+    Each timing advances every case by the same ``--steps`` steps from the same
+    state (every case is snapshotted after the warm-up and restored before each
+    phase), so the three phases do the same work, and the line says whether they
+    ended in the same bits; host wall clock around each phase, every case's last
+    call having waited for its own stream.
     The batched phase also reports the CUDA-event time of its batched CG chunks
     and their algorithmic HBM rate (80 B per edge and CG iteration, summed over
     the cases) against the measured peak.  Under
@@ -847,16 +849,26 @@ def run_batch(args, world, rank, local):
     if sampler:
         sampler.start()
     empty = {"cg_iterations": 0, "max_case_iterations": 0, "per_case_iterations": []}
+    snap = batch.snapshot()
     batch.batch_timing(reset=True)
     t_bat, st_bat = batch.advance(args.steps, batched=True) if mine else (0.0, empty)
+    fp_bat = batch.fingerprint() if mine else []
     bt = batch.batch_timing(reset=True)
     edges = [int(r.drv.layout.edge_exists.sum()) for r in batch.runs]
     per_edge = ALGO_BYTES_PER_EDGE_ITER if args.precision == "float64" else ALGO_BYTES_PER_EDGE_ITER / 2
     cg_bytes = float(sum(per_edge * e * it for e, it in zip(edges, st_bat["per_case_iterations"])))
     barrier(dist)
+    batch.restore(snap)
     t_con, st_con = batch.advance(args.steps, concurrent=True) if mine else (0.0, empty)
+    fp_con = batch.fingerprint() if mine else []
+    batch.restore(snap)
     barrier(dist)
     t_seq, st_seq = batch.advance(args.steps, concurrent=False) if mine else (0.0, empty)
+    fp_seq = batch.fingerprint() if mine else []
+    same = all(all(np.array_equal(x, y) for x, y in zip(a, b)) and all(np.array_equal(x, y) for x, y in zip(a, c))
+               for a, b, c in zip(fp_bat, fp_con, fp_seq))
+    same = -reduce_max(dist, -1.0 if same else 0.0) > 0.5   # every rank agrees
+    del snap, fp_bat, fp_con, fp_seq
     clocks = sampler.stop() if sampler else None
     launches = 0
     timing = (C.c_double * 5)()
@@ -906,6 +918,7 @@ def run_batch(args, world, rank, local):
         "concurrent": {"value": upd / con["seconds_concurrent"], "seconds": con["seconds_concurrent"],
                        "cg_iterations": int(con["cg_iterations"]),
                        "max_case_iterations": int(con["max_case_iterations"])},
+        "same_steps_bit_identical": same,
         "one_at_a_time": {"value": upd / seq["seconds_sequential"], "seconds": seq["seconds_sequential"],
                           "cg_iterations": int(seq["cg_iterations"]),
                           "max_case_iterations": int(seq["max_case_iterations"])},

@@ -167,6 +167,21 @@ class BatchRun:
             raise RuntimeError(f"case {self.cases[q].name} failed: {exc}") from exc
         return seconds, self._stats(iters)
 
+    def snapshot(self):
+        """Every case's state (``SphereRun.snapshot``)."""
+        return [r.snapshot() for r in self.runs]
+
+    def restore(self, snaps):
+        """Every case back to ``snapshot``'s state."""
+        for r, snap in zip(self.runs, snaps):
+            r.restore(snap)
+
+    def fingerprint(self):
+        """Every case's stream function, Lagrangian force and body force (host copies),
+        to compare two ways of taking the same steps."""
+        return [(np.asarray(r.s).copy(), np.asarray(r.drv.ib_force_L).copy(),
+                 np.asarray(r.loads.latest["body_force"]).copy()) for r in self.runs]
+
     def batch_timing(self, reset=True):
         """CUDA-event seconds of the batched CG chunks, batched kernels launched and
         graph captures since the last reset (pyib_batch_timing)."""

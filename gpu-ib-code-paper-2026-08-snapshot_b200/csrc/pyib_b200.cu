@@ -1856,7 +1856,7 @@ __global__ void k_dinv(long long ne, const double* __restrict__ d1, const double
 // ---------------------------------------------------------------------------
 constexpr int kBStages = 8;
 constexpr int kBatchCellDepth = 8, kBatchNodeDepth = 16;   // z planes of a batched cell / node tile
-constexpr int kBatchGroups = 4;   // cost-balanced groups of cases, parallel branches of the chunk graph
+constexpr int kBatchGroups = 8;   // cost-balanced groups of cases, parallel branches of the chunk graph
 
 struct BCase {
   Meta m;                          // the case's layout decoding and tiles, of the batch's precision

@@ -107,6 +107,26 @@ class SphereRun:
             return np.zeros(3)
         return self.motion.centre(t)
 
+    def snapshot(self):
+        """The state that the next steps start from (host copies)."""
+        return dict(s=np.asarray(self.s).copy(), s_old=np.asarray(self.s_old).copy(),
+                    state=self.drv.ib_state_dict(), step=self.step_index, time=self.drv.time,
+                    loads=np.asarray(self.loads.current).copy())
+
+    def restore(self, snap):
+        """Return to a snapshot: the following steps repeat the ones taken after it
+        bit for bit."""
+        drv = self.drv
+        self.s, self.s_old = snap["s"].copy(), snap["s_old"].copy()
+        if snap["state"] is not None:
+            drv.load_ib_state_dict(snap["state"])
+            drv.ib_force_update_count = snap["state"]["force_update_count"]
+        self.step_index, drv.time = snap["step"], snap["time"]
+        self.loads.current = snap["loads"].copy()
+        if self.motion is not None:
+            mk, vel = self.motion(drv.time)
+            drv.set_ib(drv.ib, mk, drv.ib_ds, vel)
+
     def advance(self, inner=4):
         k = self.step_index + 1
         self.drv.time = (k - 1) * self.dt
