@@ -1855,7 +1855,7 @@ __global__ void k_dinv(long long ne, const double* __restrict__ d1, const double
 // stopped (st->done) leaves its blocks idle; the host drops it from the tables.
 // ---------------------------------------------------------------------------
 constexpr int kBStages = 8;
-constexpr int kBatchCellDepth = 8, kBatchNodeDepth = 16;   // z planes of a batched cell / node tile
+constexpr int kBatchCellDepth = 16, kBatchNodeDepth = 16;   // z planes of a batched cell / node tile
 constexpr int kBatchGroups = 16;  // cost-balanced groups of cases, parallel branches of the chunk graph
 
 struct BCase {
